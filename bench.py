@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""LINPACK LU + solve on B200 — prints ONE JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lpcuda|reference]
+                    [--n 32768] [--bs 512]
+
+A step is one factorization (blocked LU without pivoting, the reference's
+lu/top/left/inner stages) plus forward/back substitution of one n x n system
+(default n = 32768, block 512, FP32: the plain FP32 workload), with the
+system's matrix restored from a pristine device copy at the start of every
+step.  ``value`` is GFLOP/s by the reference's formula 2n^3/3 + 2n^2
+(LINPACK/src/host/linpack_benchmark.hpp:509-535) over device time of K steps
+(CUDA events on the library's stream), inputs resident in HBM; ``e2e`` is the
+same metric through the C ABI host call lp_calculate (the drop-in for
+execution::pcie::calculate) with pinned host buffers: host->device copy of A
+and b, factor, solve, device->host copy of the factors and x, all inside the
+wall-clock timed call.
+
+Multi-GPU: the path does not shard (one system per GPU); under torchrun each
+rank runs an independent replica, time = max over ranks, value = total work
+of all ranks / that time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LU+solve GFLOP/s FP32 vs BF16/FP8+IR at equal residual; batched solves/s, p99 ms"
+UNIT = "GFLOP/s"
+NUM_SMS = 148
+FP32_LANES_PER_SM = 128
+
+
+def flops(n: int) -> float:
+    return 2.0 * n ** 3 / 3.0 + 2.0 * n ** 2
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        d["source"] = "measured"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0,
+            "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].isdigit():
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        sm = [int(r[1]) for r in rows]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def cpu_baseline(n: int, reps: int) -> dict:
+    """The reference's own gefa_ref_nopvt + gesl_ref_nopvt (compiled from
+    LINPACK/src/host/linpack_data.cpp into oracle/_ref/ref_bench), timed on
+    this host, on a bounded sample of the workload (same generator)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/ref_bench not built"}
+    out = subprocess.run([exe, "--n", str(n), "--reps", str(reps), "--mode", "baseline", "--seed", "42",
+                          "--margin", "1"], capture_output=True, text=True, check=True).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    return {"value": r["gflops"], "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"one n={n} system (seed 42, margin 1), best of {reps}: gefa_ref_nopvt+gesl_ref_nopvt, "
+                      f"single-threaded reference code, g++ -O3 -march=x86-64-v3; "
+                      f"residual_norm {r['residual_norm']:.3g}",
+            "t_min_s": r["t_min"], "host_nproc": os.cpu_count()}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    n = args.cpu_n
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built"}))
+        return
+    times = []
+    for i in range(args.warmup + args.steps):
+        out = subprocess.run([exe, "--n", str(n), "--reps", "1", "--mode", "baseline", "--seed", "42", "--margin",
+                              "1"], capture_output=True, text=True, check=True).stdout
+        r = json.loads(out.strip().splitlines()[-1])
+        if i >= args.warmup:
+            times.append(r["t_min"])
+    total = sum(times)
+    value = args.steps * flops(n) / total / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain FP32 LU without pivoting + solve, bounded CPU sample n={n} "
+                               f"(of the n={args.n} block-{args.bs} workload), seed 42, margin 1",
+                   "n": n, "sample_of_n": args.n, "block": args.bs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                         "sample": f"{args.steps} x one n={n} system; the reference's gefa_ref_nopvt/gesl_ref_nopvt "
+                                   "are single-threaded (no OpenMP in linpack_data.cpp), so one core is all they use"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lpcuda", choices=["lpcuda", "reference"])
+    ap.add_argument("--n", type=int, default=32768)
+    ap.add_argument("--bs", type=int, default=512)
+    ap.add_argument("--cpu-n", type=int, default=2048)
+    ap.add_argument("--cpu-reps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from hpcc_fpga_b200 import lpcuda as lp
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    n, bs = args.n, args.bs
+    ctx = lp.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+
+    A, b64, b32 = lp.generate_baseline(n, 42, 1.0)
+    with torch.cuda.stream(stream):
+        dA0 = torch.from_numpy(A).to("cuda")
+        dB0 = torch.from_numpy(b32).to("cuda")
+        dA = torch.empty_like(dA0)
+        dB = torch.empty_like(dB0)
+    torch.cuda.synchronize()
+
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+            dB.copy_(dB0)
+        ctx.gefa(dA.data_ptr(), n, n, bs)
+        ctx.gesl(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.read_profile(reset=True)
+    launches0 = ctx.read_profile(reset=False)["kernel_launches"]
+    clocks = ClockSampler(local).start()
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed = ev0.elapsed_time(ev1) * 1e-3
+    prof = ctx.read_profile(reset=True)
+    launches = prof["kernel_launches"] - launches0
+    ctx.set_profiling(False)
+    x = dB.cpu().numpy()
+    max_err = float(np.abs(x.astype(np.float64) - 1.0).max())
+    t_max = elapsed
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * args.steps * flops(n) / t_max / 1e9
+
+    # ---- roofline of the dominant kernel (the FP32 trailing update) ----
+    inner = prof["inner"]
+    achieved_tf = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    peak_tf = NUM_SMS * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
+    stage_share = {k: prof[k]["s"] / max(1e-12, sum(prof[s]["s"] for s in lp.STAGES)) for k in lp.STAGES}
+    gesl = prof["gesl"]
+    pk = peaks()
+
+    # ---- end to end through the C ABI with pinned host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        L = lp.lib()
+        pa, pb = ctypes.c_void_p(), ctypes.c_void_p()
+        lp.check(L.lp_host_alloc(ctypes.c_size_t(4 * n * n), ctypes.byref(pa)), "lp_host_alloc")
+        lp.check(L.lp_host_alloc(ctypes.c_size_t(4 * n), ctypes.byref(pb)), "lp_host_alloc")
+        hA = np.ctypeslib.as_array((ctypes.c_float * (n * n)).from_address(pa.value)).reshape(n, n)
+        hb = np.ctypeslib.as_array((ctypes.c_float * n).from_address(pb.value))
+        walls = []
+        for _ in range(1 + args.steps):
+            np.copyto(hA, A)
+            np.copyto(hb, b32)
+            if world > 1:
+                dist.barrier()
+            t0 = time.perf_counter()
+            ctx.calculate(hA, hb, bs, repetitions=1)
+            walls.append(time.perf_counter() - t0)
+        walls = walls[1:]
+        e2e_err = float(np.abs(hb.astype(np.float64) - 1.0).max())
+        wt = sum(walls)
+        if world > 1:
+            t = torch.tensor([wt], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            wt = float(t.item())
+        e2e = {"value": world * args.steps * flops(n) / wt / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": 4 * n * n + 4 * n, "d2h_bytes_per_step": 4 * n * n + 4 * n,
+               "ms_per_step": 1e3 * wt / args.steps, "max_abs_err_x": e2e_err,
+               "api": "lp_calculate (C ABI, pinned host A and b)"}
+        L.lp_host_free(pa)
+        L.lp_host_free(pb)
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"plain FP32 LU without pivoting + forward/back substitution, n={n}, block {bs}, "
+                               "1 RHS, seed 42 mt19937 diagonally dominant (margin 1), b = A*ones",
+                   "n": n, "block": bs, "precision": "f32", "rhs": 1,
+                   "l2": f"inputs larger than L2 ({4 * n * n / 2**30:.1f} GiB matrix, restored every step)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "max_abs_err_x": max_err,
+        "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)",
+                     "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": (achieved_tf / peak_tf) if achieved_tf else None,
+                     "peak_source": f"derived: {NUM_SMS} SMs x {FP32_LANES_PER_SM} FP32 lanes x 2 flop x median SM "
+                                    f"clock under load ({sm_mhz} MHz); MEASURED_PEAKS.json has no FP32 figure",
+                     "per_unit": "2*m*m*bs flop per trailing update of an m x m trailing matrix",
+                     "launches": inner["calls"], "traffic": None},
+        "stages": {k: {"s": prof[k]["s"], "share": stage_share[k], "calls": prof[k]["calls"]} for k in lp.STAGES
+                   if prof[k]["calls"]},
+        "gesl": {"s_per_step": gesl["s"] / max(1, args.steps),
+                 "GBps": gesl["bytes"] / gesl["s"] / 1e9 if gesl["s"] > 0 else None,
+                 "frac_hbm": (gesl["bytes"] / gesl["s"] / 1e9 / pk["hbm_gbs"]) if gesl["s"] > 0 else None},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if e2e is not None:
+        line["e2e"] = e2e
+    if world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(args.cpu_n, args.cpu_reps)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

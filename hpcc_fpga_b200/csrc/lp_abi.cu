@@ -1,0 +1,403 @@
+// C ABI of liblpcuda.so (declared in include/lpcuda.h): context, workspace,
+// the block-step schedule of the factorization, the substitution, and the
+// host entry points that stand in for the reference's execution backend.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "lp_common.cuh"
+#include "lp_ctx.cuh"
+
+namespace lp {
+
+static thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg) {
+    g_last_error = msg;
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof(buf), "%s failed: %s (%s) at %s:%d", what, cudaGetErrorName(e), cudaGetErrorString(e),
+                  file, line);
+    g_last_error = buf;
+    if (e == cudaErrorMemoryAllocation) return LP_E_NOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return LP_E_NODEVICE;
+    return LP_E_CUDA;
+}
+
+int Workspace::ensure(size_t bytes) {
+    if (bytes <= cap) return LP_OK;
+    if (ptr != nullptr) {
+        cudaError_t e = cudaFree(ptr);
+        ptr = nullptr;
+        cap = 0;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFree(workspace)", __FILE__, __LINE__);
+    }
+    LP_CUDA(cudaMalloc(&ptr, bytes));
+    cap = bytes;
+    return LP_OK;
+}
+
+void Workspace::release() {
+    if (ptr != nullptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+int validate_matrix(const void* a, int n, int lda, int bs, const char* who) {
+    if (a == nullptr) return fail(LP_E_INVALID, std::string(who) + ": null matrix pointer");
+    if (n <= 0) return fail(LP_E_INVALID, std::string(who) + ": n must be positive");
+    if (!is_pow2(bs) || bs < 16 || bs > 512)
+        return fail(LP_E_INVALID, std::string(who) + ": block size must be a power of two in [16, 512]");
+    if (n % bs != 0) return fail(LP_E_INVALID, std::string(who) + ": n must be a multiple of the block size");
+    if (lda < n || lda % 4 != 0)
+        return fail(LP_E_INVALID, std::string(who) + ": lda must be >= n and a multiple of 4");
+    return LP_OK;
+}
+
+static std::atomic<long long> g_launches{0};
+void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+int prof_begin(lp_ctx* c, cudaStream_t st) {
+    if (!c->prof_on) return -1;
+    if (c->prof_used + 2 > c->prof_ev.size()) {
+        for (int i = 0; i < 64; i++) {
+            cudaEvent_t e;
+            LP_CUDA(cudaEventCreate(&e));
+            c->prof_ev.push_back(e);
+        }
+    }
+    const int e0 = (int)c->prof_used++;
+    LP_CUDA(cudaEventRecord(c->prof_ev[e0], st));
+    return e0;
+}
+
+int prof_end(lp_ctx* c, cudaStream_t st, int kind, int e0, double flops, double bytes) {
+    if (e0 < 0) return LP_OK;
+    const int e1 = (int)c->prof_used++;
+    LP_CUDA(cudaEventRecord(c->prof_ev[e1], st));
+    c->marks.push_back(StageMark{kind, e0, e1, flops, bytes});
+    return LP_OK;
+}
+
+// Folds the recorded marks into the per-stage sums (waits for the stream).
+static int prof_collect(lp_ctx* c) {
+    if (c->marks.empty()) return LP_OK;
+    LP_CUDA(cudaStreamSynchronize(c->stream));
+    for (const auto& m : c->marks) {
+        float ms = 0.0f;
+        LP_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[m.e0], c->prof_ev[m.e1]));
+        c->prof_s[m.kind] += ms * 1e-3;
+        c->prof_flops[m.kind] += m.flops;
+        c->prof_bytes[m.kind] += m.bytes;
+        c->prof_calls[m.kind] += 1;
+    }
+    c->marks.clear();
+    c->prof_used = 0;
+    return LP_OK;
+}
+
+// Algorithmic work of the stages (flops; bytes of one pass over the operands).
+static double lu_flops(double b) { return 2.0 * b * b * b / 3.0; }
+static double trsm_flops(double b, double w) { return b * b * w; }
+static double inner_flops(double m, double n, double k) { return 2.0 * m * n * k; }
+static double inner_bytes(double m, double n, double k) { return 4.0 * (2.0 * m * n + k * (m + n)); }
+
+// lu stage of one diagonal block.  bs <= 128: one shared-memory kernel.
+// Larger blocks are factored as the same blocked algorithm with 128-wide
+// inner blocks (lu, top, left, inner on the bs x bs sub-matrix), which keeps
+// every piece on the kernels above and spreads the inner work over the GPU.
+static int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
+    if (bs <= 128) return launch_lu_small(d, lda, bs, st);
+    const int ib = 128;
+    float* lti = static_cast<float*>(c->lti.ptr);
+    for (int kk = 0; kk < bs / ib; kk++) {
+        float* dd = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        LP_CHECK(launch_lu_small(dd, lda, ib, st));
+        const int r = bs - (kk + 1) * ib;
+        if (r <= 0) break;
+        LP_CHECK(launch_trsm_top(dd, lda, dd + ib, lda, ib, r, st));
+        LP_CHECK(launch_trsm_left(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, st));
+        LP_CHECK(launch_sgemm_update(dd + (size_t)ib * lda + ib, lda, lti, r, dd + ib, lda, r, r, ib, st));
+    }
+    return LP_OK;
+}
+
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
+    LP_CHECK(c->lt.ensure(sizeof(float) * (size_t)bs * n));
+    if (bs > 128) LP_CHECK(c->lti.ensure(sizeof(float) * (size_t)128 * bs));
+    float* lt = static_cast<float*>(c->lt.ptr);
+    const int nb = n / bs;
+    const double b = bs;
+    for (int K = 0; K < nb; K++) {
+        float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+        int e = prof_begin(c, st);
+        LP_CHECK(lu_stage(c, d, lda, bs, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_LU, e, lu_flops(b), 8.0 * b * b));
+        const int rest = n - (K + 1) * bs;
+        if (rest <= 0) break;
+        const double r = rest;
+        e = prof_begin(c, st);
+        LP_CHECK(launch_trsm_top(d, lda, d + bs, lda, bs, rest, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, trsm_flops(b, r), 8.0 * b * r));
+        e = prof_begin(c, st);
+        LP_CHECK(launch_trsm_left(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
+        e = prof_begin(c, st);
+        LP_CHECK(launch_sgemm_update(d + (size_t)bs * lda + bs, lda, lt, rest, d + bs, lda, rest, rest, bs, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(r, r, b), inner_bytes(r, r, b)));
+    }
+    return LP_OK;
+}
+
+int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st) {
+    LP_CHECK(c->gw.ensure(sizeof(float) * gesl_work_floats(n, nrhs)));
+    const int e = prof_begin(c, st);
+    LP_CHECK(launch_gesl(dLU, lda, n, dB, ldb, nrhs, static_cast<float*>(c->gw.ptr), st));
+    const double nn = n;
+    return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
+}
+
+static float elapsed_s(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms * 1e-3f;
+}
+
+}  // namespace lp
+
+using namespace lp;
+
+extern "C" {
+
+const char* lp_strerror(int status) {
+    switch (status) {
+        case LP_OK: return "ok";
+        case LP_E_INVALID: return "invalid argument";
+        case LP_E_CUDA: return "CUDA error";
+        case LP_E_NOMEM: return "out of memory";
+        case LP_E_TIMEOUT: return "timeout";
+        case LP_E_NUMERIC: return "non-finite result";
+        case LP_E_STATE: return "invalid state";
+        case LP_E_BUDGET: return "device-memory budget exceeded";
+        case LP_E_NODEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+const char* lp_last_error(void) { return g_last_error.c_str(); }
+
+int lp_version(void) { return LPCUDA_VERSION; }
+
+int lp_device_count(int* count) {
+    if (count == nullptr) return fail(LP_E_INVALID, "lp_device_count: null output");
+    *count = 0;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "cudaGetDeviceCount", __FILE__, __LINE__) == LP_E_CUDA ? LP_E_NODEVICE : LP_E_NODEVICE;
+    }
+    *count = n;
+    return LP_OK;
+}
+
+int lp_ctx_create(int device, lp_ctx** out) {
+    if (out == nullptr) return fail(LP_E_INVALID, "lp_ctx_create: null output");
+    *out = nullptr;
+    int count = 0;
+    LP_CHECK(lp_device_count(&count));
+    if (device < 0 || device >= count) return fail(LP_E_NODEVICE, "lp_ctx_create: no such CUDA device");
+    LP_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    LP_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+        return fail(LP_E_NODEVICE, std::string("lp_ctx_create: device '") + prop.name +
+                                       "' is not sm_100 (this library is built for sm_100a only)");
+    LP_CHECK(lu_init_attrs());
+    LP_CHECK(trsm_init_attrs());
+    LP_CHECK(sgemm_init_attrs());
+    LP_CHECK(gesl_init_attrs());
+    lp_ctx* c = new lp_ctx();
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    std::snprintf(c->name, sizeof(c->name), "%s", prop.name);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        lp_ctx_destroy(c);
+        return cuda_fail(e, "lp_ctx_create: stream/event creation", __FILE__, __LINE__);
+    }
+    *out = c;
+    return LP_OK;
+}
+
+int lp_ctx_destroy(lp_ctx* c) {
+    if (c == nullptr) return LP_OK;
+    cudaSetDevice(c->device);
+    if (c->stream != nullptr) cudaStreamSynchronize(c->stream);
+    c->release_all();
+    for (int i = 0; i < 8; i++)
+        if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
+    if (c->stream != nullptr) cudaStreamDestroy(c->stream);
+    delete c;
+    return LP_OK;
+}
+
+int lp_ctx_stream(lp_ctx* c, void** stream) {
+    if (c == nullptr || stream == nullptr) return fail(LP_E_INVALID, "lp_ctx_stream: null argument");
+    *stream = c->stream;
+    return LP_OK;
+}
+
+int lp_ctx_sync(lp_ctx* c) {
+    if (c == nullptr) return fail(LP_E_INVALID, "lp_ctx_sync: null context");
+    LP_CUDA(cudaSetDevice(c->device));
+    LP_CUDA(cudaStreamSynchronize(c->stream));
+    return LP_OK;
+}
+
+int lp_ctx_device_name(lp_ctx* c, char* buf, int buflen) {
+    if (c == nullptr || buf == nullptr || buflen <= 0) return fail(LP_E_INVALID, "lp_ctx_device_name: bad argument");
+    std::snprintf(buf, (size_t)buflen, "%s", c->name);
+    return LP_OK;
+}
+
+int lp_ctx_set_profiling(lp_ctx* c, int on) {
+    if (c == nullptr) return fail(LP_E_INVALID, "lp_ctx_set_profiling: null context");
+    c->prof_on = on != 0;
+    return LP_OK;
+}
+
+int lp_ctx_read_profile(lp_ctx* c, lp_profile* out, int reset) {
+    if (c == nullptr || out == nullptr) return fail(LP_E_INVALID, "lp_ctx_read_profile: null argument");
+    LP_CUDA(cudaSetDevice(c->device));
+    LP_CHECK(prof_collect(c));
+    for (int k = 0; k < LP_NSTAGES; k++) {
+        out->stage_s[k] = c->prof_s[k];
+        out->stage_flops[k] = c->prof_flops[k];
+        out->stage_bytes[k] = c->prof_bytes[k];
+        out->stage_calls[k] = c->prof_calls[k];
+        if (reset) {
+            c->prof_s[k] = c->prof_flops[k] = c->prof_bytes[k] = 0.0;
+            c->prof_calls[k] = 0;
+        }
+    }
+    out->kernel_launches = launch_count();
+    return LP_OK;
+}
+
+int lp_host_alloc(size_t bytes, void** out) {
+    if (out == nullptr || bytes == 0) return fail(LP_E_INVALID, "lp_host_alloc: bad argument");
+    *out = nullptr;
+    LP_CUDA(cudaHostAlloc(out, bytes, cudaHostAllocPortable));
+    return LP_OK;
+}
+
+int lp_host_free(void* p) {
+    if (p == nullptr) return LP_OK;
+    LP_CUDA(cudaFreeHost(p));
+    return LP_OK;
+}
+
+// ---- block stages -----------------------------------------------------------
+int lp_lu_block_dev(lp_ctx* c, float* dA, int lda, int bs) {
+    if (c == nullptr || dA == nullptr) return fail(LP_E_INVALID, "lp_lu_block_dev: null argument");
+    if (!is_pow2(bs) || bs < 16 || bs > 512 || lda < bs || lda % 4 != 0)
+        return fail(LP_E_INVALID, "lp_lu_block_dev: bs must be a power of two in [16, 512], lda >= bs, lda % 4 == 0");
+    LP_CUDA(cudaSetDevice(c->device));
+    if (bs > 128) LP_CHECK(c->lti.ensure(sizeof(float) * (size_t)128 * bs));
+    return lu_stage(c, dA, lda, bs, c->stream);
+}
+
+int lp_top_update_dev(lp_ctx* c, const float* dLU, int ldlu, float* dT, int ldt, int bs, int ncols) {
+    if (c == nullptr || dLU == nullptr || dT == nullptr) return fail(LP_E_INVALID, "lp_top_update_dev: null argument");
+    if (ncols < 0 || ldt < ncols || ldlu < bs) return fail(LP_E_INVALID, "lp_top_update_dev: bad sizes");
+    LP_CUDA(cudaSetDevice(c->device));
+    return launch_trsm_top(dLU, ldlu, dT, ldt, bs, ncols, c->stream);
+}
+
+int lp_left_update_dev(lp_ctx* c, const float* dLU, int ldlu, float* dL, int ldl, int bs, int nrows, float* dLt,
+                       int ldlt) {
+    if (c == nullptr || dLU == nullptr || dL == nullptr) return fail(LP_E_INVALID, "lp_left_update_dev: null argument");
+    if (nrows < 0 || ldl < bs || ldlu < bs || (dLt != nullptr && ldlt < nrows))
+        return fail(LP_E_INVALID, "lp_left_update_dev: bad sizes");
+    LP_CUDA(cudaSetDevice(c->device));
+    return launch_trsm_left(dLU, ldlu, dL, ldl, bs, nrows, dLt, ldlt, c->stream);
+}
+
+int lp_inner_update_dev(lp_ctx* c, float* dC, int ldc, const float* dLt, int ldlt, const float* dT, int ldt, int m,
+                        int n, int bs) {
+    if (c == nullptr || dC == nullptr || dLt == nullptr || dT == nullptr)
+        return fail(LP_E_INVALID, "lp_inner_update_dev: null argument");
+    if (m < 0 || n < 0 || ldc < n || ldlt < m || ldt < n) return fail(LP_E_INVALID, "lp_inner_update_dev: bad sizes");
+    LP_CUDA(cudaSetDevice(c->device));
+    return launch_sgemm_update(dC, ldc, dLt, ldlt, dT, ldt, m, n, bs, c->stream);
+}
+
+// ---- whole factorization / solve ------------------------------------------------
+int lp_gefa_dev(lp_ctx* c, float* dA, int n, int lda, int bs) {
+    if (c == nullptr) return fail(LP_E_INVALID, "lp_gefa_dev: null context");
+    LP_CHECK(validate_matrix(dA, n, lda, bs, "lp_gefa_dev"));
+    if (!aligned16(dA)) return fail(LP_E_INVALID, "lp_gefa_dev: matrix must be 16-byte aligned");
+    LP_CUDA(cudaSetDevice(c->device));
+    return gefa_f32(c, dA, n, lda, bs, c->stream);
+}
+
+int lp_gesl_dev(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb) {
+    if (c == nullptr || dLU == nullptr || dB == nullptr) return fail(LP_E_INVALID, "lp_gesl_dev: null argument");
+    if (n <= 0 || lda < n || nrhs <= 0 || ldb < n) return fail(LP_E_INVALID, "lp_gesl_dev: bad sizes");
+    LP_CUDA(cudaSetDevice(c->device));
+    return gesl_f32(c, dLU, n, lda, dB, nrhs, ldb, c->stream);
+}
+
+// ---- host entry points --------------------------------------------------------------
+int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, float* b, double* gefa_times,
+                 double* gesl_times) {
+    if (c == nullptr || b == nullptr || gefa_times == nullptr || gesl_times == nullptr)
+        return fail(LP_E_INVALID, "lp_calculate: null argument");
+    LP_CHECK(validate_matrix(A, n, lda, bs, "lp_calculate"));
+    if (repetitions <= 0) return fail(LP_E_INVALID, "lp_calculate: repetitions must be positive");
+    LP_CUDA(cudaSetDevice(c->device));
+    const size_t abytes = sizeof(float) * (size_t)n * lda;
+    LP_CHECK(c->dA.ensure(abytes));
+    LP_CHECK(c->dB.ensure(sizeof(float) * (size_t)n));
+    float* dA = static_cast<float*>(c->dA.ptr);
+    float* dB = static_cast<float*>(c->dB.ptr);
+    cudaStream_t st = c->stream;
+    for (int rep = 0; rep < repetitions; rep++) {
+        LP_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, st));
+        LP_CUDA(cudaMemcpyAsync(dB, b, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+        LP_CUDA(cudaEventRecord(c->ev[0], st));
+        LP_CHECK(gefa_f32(c, dA, n, lda, bs, st));
+        LP_CUDA(cudaEventRecord(c->ev[1], st));
+        LP_CHECK(gesl_f32(c, dA, n, lda, dB, 1, n, st));
+        LP_CUDA(cudaEventRecord(c->ev[2], st));
+        LP_CUDA(cudaStreamSynchronize(st));
+        gefa_times[rep] = elapsed_s(c->ev[0], c->ev[1]);
+        gesl_times[rep] = elapsed_s(c->ev[1], c->ev[2]);
+    }
+    LP_CUDA(cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaMemcpyAsync(b, dB, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    return LP_OK;
+}
+
+int lp_solve_host(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
+                  double* x, int max_iters, lp_timing* t) {
+    if (c == nullptr || b64 == nullptr || x == nullptr) return fail(LP_E_INVALID, "lp_solve_host: null argument");
+    LP_CHECK(validate_matrix(A, n, lda, bs, "lp_solve_host"));
+    if (nrhs <= 0) return fail(LP_E_INVALID, "lp_solve_host: nrhs must be positive");
+    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR)
+        return fail(LP_E_INVALID, "lp_solve_host: unknown precision");
+    LP_CUDA(cudaSetDevice(c->device));
+    return solve_host_impl(c, precision, n, bs, A, lda, b64, nrhs, x, max_iters, t);
+}
+
+}  // extern "C"

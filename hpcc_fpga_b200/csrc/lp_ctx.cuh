@@ -1,0 +1,61 @@
+// The lp_ctx object behind the opaque handle of include/lpcuda.h.
+#pragma once
+
+#include <vector>
+
+#include "lp_common.cuh"
+
+namespace lp {
+
+// One profiled stage launch: events e0/e1 of the context's pool bracket it.
+struct StageMark {
+    int kind;
+    int e0, e1;
+    double flops, bytes;
+};
+
+// A device allocation that only grows (freed on growth and at destroy).
+struct Workspace {
+    void* ptr = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);
+    void release();
+};
+
+int validate_matrix(const void* a, int n, int lda, int bs, const char* who);
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st);
+int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
+int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
+                    double* x, int max_iters, lp_timing* t);
+
+// Stage profiling: prof_begin returns an event index (or -1 when profiling
+// is off); prof_end records the closing event and the stage's work.
+int prof_begin(lp_ctx* c, cudaStream_t st);
+int prof_end(lp_ctx* c, cudaStream_t st, int kind, int e0, double flops, double bytes);
+
+}  // namespace lp
+
+struct lp_ctx {
+    int device = 0;
+    int num_sms = 0;
+    char name[256] = {0};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {nullptr};
+    lp::Workspace lt;    // transposed left panel (bs x n)
+    lp::Workspace lti;   // transposed inner left panel of the recursive lu stage
+    lp::Workspace gw;    // substitution work vectors
+    lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
+    lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
+    bool prof_on = false;
+    std::vector<cudaEvent_t> prof_ev;         // event pool, reused after every read
+    size_t prof_used = 0;
+    std::vector<lp::StageMark> marks;
+    double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
+    long long prof_calls[LP_NSTAGES] = {0};
+    void release_all() {
+        lp::Workspace* all[] = {&lt, &lti, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
+        for (auto* w : all) w->release();
+        for (auto e : prof_ev) cudaEventDestroy(e);
+        prof_ev.clear();
+    }
+};

@@ -1,0 +1,249 @@
+"""ctypes binding of liblpcuda.so (the C ABI declared in include/lpcuda.h).
+
+This module only marshals arguments; all work is done by the CUDA library.
+It raises if the library is missing — there is no fallback path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "_lib", "liblpcuda.so")
+HEADER_PATH = os.path.join(os.path.dirname(_PKG), "include", "lpcuda.h")
+
+LP_OK = 0
+LP_E_INVALID = -1
+LP_E_CUDA = -2
+LP_E_NOMEM = -3
+LP_E_TIMEOUT = -4
+LP_E_NUMERIC = -5
+LP_E_STATE = -6
+LP_E_BUDGET = -7
+LP_E_NODEVICE = -8
+
+LP_F32, LP_BF16_IR, LP_FP8_IR = 0, 1, 2
+PRECISIONS = {"f32": LP_F32, "bf16": LP_BF16_IR, "fp8": LP_FP8_IR}
+
+_F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_VP = ctypes.c_void_p
+_I = ctypes.c_int
+
+
+class LpTiming(ctypes.Structure):
+    _fields_ = [("gefa_s", ctypes.c_double), ("gesl_s", ctypes.c_double), ("ir_s", ctypes.c_double),
+                ("h2d_s", ctypes.c_double), ("d2h_s", ctypes.c_double), ("ir_iters", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("hpl_resid", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_ if f[0] != "reserved"}
+
+
+STAGES = ["lu", "top", "left", "inner", "gesl", "other"]
+
+
+class LpProfile(ctypes.Structure):
+    _fields_ = [("stage_s", ctypes.c_double * 6), ("stage_flops", ctypes.c_double * 6),
+                ("stage_bytes", ctypes.c_double * 6), ("stage_calls", ctypes.c_longlong * 6),
+                ("kernel_launches", ctypes.c_longlong)]
+
+    def as_dict(self) -> dict:
+        d = {s: {"s": self.stage_s[i], "flops": self.stage_flops[i], "bytes": self.stage_bytes[i],
+                 "calls": self.stage_calls[i]} for i, s in enumerate(STAGES)}
+        d["kernel_launches"] = self.kernel_launches
+        return d
+
+
+class LpError(RuntimeError):
+    def __init__(self, status: int, where: str, detail: str):
+        self.status = status
+        super().__init__(f"{where}: {strerror(status)} ({status}): {detail}")
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load liblpcuda.so (built by hpcc_fpga_b200.build); raise if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m hpcc_fpga_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    L.lp_strerror.restype = ctypes.c_char_p
+    L.lp_strerror.argtypes = [_I]
+    L.lp_last_error.restype = ctypes.c_char_p
+    L.lp_last_error.argtypes = []
+    L.lp_version.restype = _I
+    L.lp_device_count.argtypes = [ctypes.POINTER(_I)]
+    L.lp_ctx_create.argtypes = [_I, ctypes.POINTER(_VP)]
+    L.lp_ctx_destroy.argtypes = [_VP]
+    L.lp_ctx_stream.argtypes = [_VP, ctypes.POINTER(_VP)]
+    L.lp_ctx_sync.argtypes = [_VP]
+    L.lp_ctx_device_name.argtypes = [_VP, ctypes.c_char_p, _I]
+    L.lp_ctx_set_profiling.argtypes = [_VP, _I]
+    L.lp_ctx_read_profile.argtypes = [_VP, ctypes.POINTER(LpProfile), _I]
+    L.lp_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(_VP)]
+    L.lp_host_free.argtypes = [_VP]
+    L.lp_lu_block_dev.argtypes = [_VP, _VP, _I, _I]
+    L.lp_top_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _I, _I]
+    L.lp_left_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _I, _I, _VP, _I]
+    L.lp_inner_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _VP, _I, _I, _I, _I]
+    L.lp_gefa_dev.argtypes = [_VP, _VP, _I, _I, _I]
+    L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
+    L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
+    L.lp_solve_host.argtypes = [_VP, _I, _I, _I, _F32P, _I, _F64P, _I, _F64P, _I, ctypes.POINTER(LpTiming)]
+    L.lp_generate_reference.argtypes = [_F32P, _F32P, _I, _I, ctypes.POINTER(ctypes.c_float),
+                                        ctypes.POINTER(ctypes.c_float)]
+    L.lp_generate_baseline.argtypes = [_F32P, _VP, _VP, _I, ctypes.c_uint, ctypes.c_double]
+    _lib = L
+    return L
+
+
+def strerror(status: int) -> str:
+    return lib().lp_strerror(status).decode()
+
+
+def last_error() -> str:
+    return lib().lp_last_error().decode()
+
+
+def check(status: int, where: str) -> None:
+    if status != LP_OK:
+        raise LpError(status, where, last_error())
+
+
+def header_functions(path: str = HEADER_PATH) -> list[str]:
+    """Names of the functions include/lpcuda.h declares."""
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(lp_[a-z0-9_]+)\s*\(", text)))
+
+
+def device_count() -> int:
+    n = _I(0)
+    st = lib().lp_device_count(ctypes.byref(n))
+    return n.value if st == LP_OK else 0
+
+
+# ------------------------------------------------------------------ generators
+def generate_reference(n: int, diag_dominant: bool = True):
+    """LinpackBenchmark::generateInputData (one rank): (A, b, norma, normb)."""
+    A = np.empty((n, n), np.float32)
+    b = np.empty(n, np.float32)
+    na, nb = ctypes.c_float(), ctypes.c_float()
+    check(lib().lp_generate_reference(A, b, n, int(diag_dominant), ctypes.byref(na), ctypes.byref(nb)),
+          "lp_generate_reference")
+    return A, b, float(na.value), float(nb.value)
+
+
+def generate_baseline(n: int, seed: int = 42, margin: float = 1.0):
+    """Seeded workload matrix: (A float32, b64 float64, b32 float32)."""
+    A = np.empty((n, n), np.float32)
+    b64 = np.empty(n, np.float64)
+    b32 = np.empty(n, np.float32)
+    check(lib().lp_generate_baseline(A, b64.ctypes.data, b32.ctypes.data, n, seed, float(margin)),
+          "lp_generate_baseline")
+    return A, b64, b32
+
+
+# ------------------------------------------------------------------ context
+class Context:
+    """One CUDA device, stream and workspace (lp_ctx)."""
+
+    def __init__(self, device: int = 0):
+        h = _VP()
+        check(lib().lp_ctx_create(device, ctypes.byref(h)), "lp_ctx_create")
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().lp_ctx_destroy(self._h)
+            self._h = _VP()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        s = _VP()
+        check(lib().lp_ctx_stream(self._h, ctypes.byref(s)), "lp_ctx_stream")
+        return s.value or 0
+
+    def sync(self) -> None:
+        check(lib().lp_ctx_sync(self._h), "lp_ctx_sync")
+
+    def device_name(self) -> str:
+        buf = ctypes.create_string_buffer(256)
+        check(lib().lp_ctx_device_name(self._h, buf, 256), "lp_ctx_device_name")
+        return buf.value.decode()
+
+    def set_profiling(self, on: bool) -> None:
+        check(lib().lp_ctx_set_profiling(self._h, int(on)), "lp_ctx_set_profiling")
+
+    def read_profile(self, reset: bool = True) -> dict:
+        p = LpProfile()
+        check(lib().lp_ctx_read_profile(self._h, ctypes.byref(p), int(reset)), "lp_ctx_read_profile")
+        return p.as_dict()
+
+    # ---- device-pointer entry points (pointers as ints) -----------------
+    def lu_block(self, dA: int, lda: int, bs: int) -> None:
+        check(lib().lp_lu_block_dev(self._h, dA, lda, bs), "lp_lu_block_dev")
+
+    def top_update(self, dLU: int, ldlu: int, dT: int, ldt: int, bs: int, ncols: int) -> None:
+        check(lib().lp_top_update_dev(self._h, dLU, ldlu, dT, ldt, bs, ncols), "lp_top_update_dev")
+
+    def left_update(self, dLU: int, ldlu: int, dL: int, ldl: int, bs: int, nrows: int,
+                    dLt: int | None = None, ldlt: int = 0) -> None:
+        check(lib().lp_left_update_dev(self._h, dLU, ldlu, dL, ldl, bs, nrows, dLt, ldlt), "lp_left_update_dev")
+
+    def inner_update(self, dC: int, ldc: int, dLt: int, ldlt: int, dT: int, ldt: int, m: int, n: int,
+                     bs: int) -> None:
+        check(lib().lp_inner_update_dev(self._h, dC, ldc, dLt, ldlt, dT, ldt, m, n, bs), "lp_inner_update_dev")
+
+    def gefa(self, dA: int, n: int, lda: int, bs: int) -> None:
+        check(lib().lp_gefa_dev(self._h, dA, n, lda, bs), "lp_gefa_dev")
+
+    def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
+        check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")
+
+    # ---- host entry points ------------------------------------------------
+    def calculate(self, A: np.ndarray, b: np.ndarray, bs: int, repetitions: int = 1):
+        """execution::pcie::calculate stand-in: factors A in place, b -> x.
+        Returns {"gefa": [...], "gesl": [...]} in seconds."""
+        n = A.shape[0]
+        tg = np.zeros(repetitions, np.float64)
+        ts = np.zeros(repetitions, np.float64)
+        check(lib().lp_calculate(self._h, n, A.shape[1], bs, repetitions, A, b, tg, ts), "lp_calculate")
+        return {"gefa": tg.tolist(), "gesl": ts.tolist()}
+
+    def solve_host(self, A: np.ndarray, b64: np.ndarray, bs: int, precision: str = "f32",
+                   max_iters: int = 0):
+        """Factor + solve (+ FP64 refinement).  b64: (n,) or (nrhs, n)."""
+        A = np.ascontiguousarray(A, dtype=np.float32)
+        B = np.ascontiguousarray(np.atleast_2d(b64), dtype=np.float64)
+        nrhs, n = B.shape
+        x = np.empty_like(B)
+        t = LpTiming()
+        check(lib().lp_solve_host(self._h, PRECISIONS[precision], n, bs, A, A.shape[1], B, nrhs, x, max_iters,
+                                  ctypes.byref(t)), "lp_solve_host")
+        return (x[0] if np.ndim(b64) == 1 else x), t.as_dict()

@@ -1,0 +1,184 @@
+/*
+ * lpcuda — B200 (sm_100a) LINPACK LU-without-pivoting + substitution.
+ *
+ * C ABI of liblpcuda.so: plain pointers and sizes, no C++ types, no
+ * exceptions.  Every entry point returns an int status (LP_OK = 0, < 0 on
+ * error); lp_strerror() names it and lp_last_error() gives the detail of the
+ * last failure on the calling thread.
+ *
+ * Matrix convention (identical to HPCC_FPGA LINPACK): a matrix is a flat
+ * array a[] with leading dimension lda; the factored matrix is
+ * M(i,j) = a[j*lda + i]; b = M * ones.  After factorization a[] holds the
+ * reference's encoding (LINPACK/src/host/linpack_data.cpp:166-196): the
+ * diagonal holds -1/u_kk, storage row k right of the diagonal the negated
+ * multipliers, storage column k below the diagonal U, unscaled.
+ *
+ * Functions named *_dev take device pointers and are ordered on the
+ * context's CUDA stream (lp_ctx_stream); the others take host pointers and
+ * return after the work is done.
+ */
+#ifndef LPCUDA_H
+#define LPCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LPCUDA_VERSION 100
+
+/* Status codes. */
+#define LP_OK 0
+#define LP_E_INVALID (-1)   /* bad argument (size, block size, alignment, null) */
+#define LP_E_CUDA (-2)      /* a CUDA runtime call failed */
+#define LP_E_NOMEM (-3)     /* device or host allocation failed */
+#define LP_E_TIMEOUT (-4)   /* a bounded wait expired */
+#define LP_E_NUMERIC (-5)   /* non-finite pivot or result */
+#define LP_E_STATE (-6)     /* call not valid in the object's current state */
+#define LP_E_BUDGET (-7)    /* request exceeds the device-memory budget */
+#define LP_E_NODEVICE (-8)  /* no CUDA device / driver */
+
+/* Factorization precision.  LP_F32: every stage in FP32 (the reference's
+ * single-precision build).  LP_BF16_IR / LP_FP8_IR: the trailing (inner)
+ * update runs on the tensor cores with operands rounded to BF16 or to FP8
+ * E4M3 with one absmax scale per 512x512 block, FP32 accumulation; the
+ * diagonal-block LU and the triangular updates stay FP32; the solve is
+ * refined in FP64 (residual and update) until the HPL scaled residual is
+ * at most 16. */
+typedef enum { LP_F32 = 0, LP_BF16_IR = 1, LP_FP8_IR = 2 } lp_precision;
+
+typedef struct lp_ctx lp_ctx;
+
+/* Timing and accuracy of one factor/solve, filled by the host entry points. */
+typedef struct {
+    double gefa_s;     /* factorization, device time (CUDA events) */
+    double gesl_s;     /* forward + back substitution, device time */
+    double ir_s;       /* refinement loop (residual + solves + update), device time */
+    double h2d_s;      /* host->device copies */
+    double d2h_s;      /* device->host copies */
+    int ir_iters;      /* refinement iterations (0 for LP_F32) */
+    int reserved;
+    double hpl_resid;  /* HPL scaled residual of the returned x (eps = DBL_EPSILON/2), or -1 */
+} lp_timing;
+
+/* ---- errors ------------------------------------------------------------ */
+const char* lp_strerror(int status);
+/* Detail of the last failure on the calling thread ("" if none). */
+const char* lp_last_error(void);
+int lp_version(void);
+
+/* ---- context ------------------------------------------------------------
+ * Replaces the OpenCL device/context/program setup of the harness
+ * (shared/include/hpcc_benchmark.hpp:560-575, shared/setup/fpga_setup.cpp)
+ * with one CUDA device, stream and workspace. */
+int lp_device_count(int* count);
+int lp_ctx_create(int device, lp_ctx** out);
+int lp_ctx_destroy(lp_ctx* ctx);
+/* The cudaStream_t the *_dev calls are ordered on (as void*). */
+int lp_ctx_stream(lp_ctx* ctx, void** stream);
+int lp_ctx_sync(lp_ctx* ctx);
+/* Name of the device ("NVIDIA B200"), for the JSON "device" key
+ * (hpcc_benchmark.hpp:501 getDeviceName). */
+int lp_ctx_device_name(lp_ctx* ctx, char* buf, int buflen);
+/* Page-locked host memory for matrices and vectors (the reference allocates
+ * them 4096-aligned with posix_memalign, linpack_data.hpp:196-198); pinned
+ * buffers make the host<->device copies of lp_calculate run at full speed. */
+int lp_host_alloc(size_t bytes, void** out);
+int lp_host_free(void* p);
+
+/* ---- profiling -------------------------------------------------------------
+ * Per-stage device times (CUDA events recorded around every stage launch on
+ * the context's stream while profiling is on) and the algorithmic work of
+ * those launches; replaces the reference's std::chrono wall clocks around
+ * the whole loop (execution_pcie.hpp:158-169,649-669). */
+#define LP_STAGE_LU 0
+#define LP_STAGE_TOP 1
+#define LP_STAGE_LEFT 2
+#define LP_STAGE_INNER 3
+#define LP_STAGE_GESL 4
+#define LP_STAGE_OTHER 5
+#define LP_NSTAGES 6
+typedef struct {
+    double stage_s[LP_NSTAGES];      /* summed device time per stage */
+    double stage_flops[LP_NSTAGES];  /* algorithmic flops of those launches */
+    double stage_bytes[LP_NSTAGES];  /* algorithmic HBM bytes of those launches */
+    long long stage_calls[LP_NSTAGES];
+    long long kernel_launches;       /* kernels launched through this library by the process (cumulative) */
+} lp_profile;
+int lp_ctx_set_profiling(lp_ctx* ctx, int on);
+/* Waits for the context's stream, fills out, and clears the stage sums if reset. */
+int lp_ctx_read_profile(lp_ctx* ctx, lp_profile* out, int reset);
+
+/* ---- block stages (device pointers) -------------------------------------
+ * The four kernels of LINPACK/src/device/hpl_torus_PCIE.cl, as whole-panel
+ * launches.  bs is the block size (power of two, 16..512). */
+
+/* lu: factor the bs x bs diagonal block at dA in place
+ * (hpl_torus_PCIE.cl:211-446; arithmetic of linpack_data.cpp:166-196). */
+int lp_lu_block_dev(lp_ctx* ctx, float* dA, int lda, int bs);
+/* top: update the bs x ncols block row right of a factored diagonal block
+ * (hpl_torus_PCIE.cl:452-582; host loop test_kernel_communication.cpp:776-789). */
+int lp_top_update_dev(lp_ctx* ctx, const float* dLU, int ldlu, float* dT, int ldt, int bs, int ncols);
+/* left: update the nrows x bs block column below a factored diagonal block
+ * (hpl_torus_PCIE.cl:588-709; host loop test_kernel_communication.cpp:624-631).
+ * If dLt is not NULL the result is also written transposed (dLt[k*ldlt + r]),
+ * the operand layout of the inner update (the reference's left_block copy,
+ * hpl_torus_PCIE.cl:697-708). */
+int lp_left_update_dev(lp_ctx* ctx, const float* dLU, int ldlu, float* dL, int ldl, int bs, int nrows,
+                       float* dLt, int ldlt);
+/* inner: C(m x n) += L(m x bs) * T(bs x n), FP32
+ * (inner_update_mm, hpl_torus_PCIE.cl:711-865).  L is given transposed
+ * (dLt: bs x m, leading dimension ldlt). */
+int lp_inner_update_dev(lp_ctx* ctx, float* dC, int ldc, const float* dLt, int ldlt, const float* dT, int ldt,
+                        int m, int n, int bs);
+
+/* ---- whole factorization and solve (device pointers) -------------------- */
+/* Blocked right-looking LU without pivoting of the n x n matrix at dA, in
+ * place, in the reference encoding.  Replaces the block-row loop of
+ * execution::pcie::calculate (execution_types/execution_pcie.hpp:177-641).
+ * n must be a multiple of bs. */
+int lp_gefa_dev(lp_ctx* ctx, float* dA, int n, int lda, int bs);
+/* Forward + back substitution with the encoded factors for nrhs right-hand
+ * sides stored as rows of dB (dB[r*ldb + i]); the solutions overwrite dB.
+ * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229). */
+int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb);
+
+/* ---- host entry points --------------------------------------------------- */
+/* The CUDA execution backend: the drop-in for
+ *   std::map<std::string, std::vector<double>> execution::pcie::calculate(
+ *       const ExecutionSettings<LinpackProgramSettings,...>&, LinpackData&)
+ * (LINPACK/src/host/execution_types/execution_pcie.hpp:53-728), selected by
+ * LinpackBenchmark::executeKernel (linpack_benchmark.hpp:306-324).
+ * For each of `repetitions`: upload A and b (untimed, execution_pcie.hpp:123-127),
+ * factor (timed -> gefa_times[rep]), solve on the device (timed ->
+ * gesl_times[rep]).  On return A holds the factors (execution_pcie.hpp:695-696)
+ * and, unlike the reference (whose GESL runs on the host afterwards,
+ * linpack_benchmark.hpp:321-323), b holds the solution x. */
+int lp_calculate(lp_ctx* ctx, int n, int lda, int bs, int repetitions, float* A, float* b,
+                 double* gefa_times, double* gesl_times);
+
+/* Factor a host matrix in place and solve for host right-hand sides, with
+ * the chosen precision; copies are part of the call and are timed in t.
+ * For LP_F32, x = the FP32 solve widened to double; for the mixed
+ * precisions, x is refined in FP64 against b64 (FP64 right-hand sides,
+ * rows of length n) until the HPL scaled residual is <= 16 or max_iters. */
+int lp_solve_host(lp_ctx* ctx, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
+                  double* x, int max_iters, lp_timing* t);
+
+/* ---- input generation (host only, no GPU needed) ------------------------ */
+/* LinpackBenchmark::generateInputData for one rank
+ * (LINPACK/src/host/linpack_benchmark.hpp:211-297): mt19937(0),
+ * uniform_real_distribution<double>(0,1) narrowed to float; diagonal =
+ * storage-row sum when diag_dominant; b = storage-column sums. */
+int lp_generate_reference(float* A, float* b, int n, int diag_dominant, float* norma, float* normb);
+/* Seeded benchmark-workload generator: mt19937(seed), entries
+ * (u>>8)*2^-24 - 0.5; diagonal = sum|off-diagonal| + margin; b64 = M*ones in
+ * FP64 (exact), b32 = (float)b64.  Either output pointer may be NULL. */
+int lp_generate_baseline(float* A, double* b64, float* b32, int n, unsigned seed, double margin);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LPCUDA_H */

@@ -1,0 +1,119 @@
+"""Whole factorization + substitution on the GPU against the oracle.
+
+Mirrors LINPACK/tests/test_kernel_functionality_and_host_integration.cpp:
+executeKernel on 1, 2 and 3 blocks (:128-131) must give |x_i - 1| < 1e-3 for
+every i (:43-48) and pass validateOutput (residn < 1,
+linpack_benchmark.hpp:416-417,465); the factors must agree with
+gefa_ref_nopvt (the disabled GEFA test, :53-74, tolerance 1e-3).  Tighter
+bounds are stated per test."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+FLT_EPS = float(np.finfo(np.float32).eps)
+
+
+@pytest.mark.parametrize("bs", [16, 32, 128, 512])
+@pytest.mark.parametrize("blocks", [1, 2, 3])
+def test_calculate_reference_inputs(ctx, bs, blocks):
+    n = bs * blocks
+    A, b, _, normb = oracle.gen_reference(n)
+    A_dev, b_dev = A.copy(), b.copy()
+    t = ctx.calculate(A_dev, b_dev, bs, repetitions=1)
+    assert len(t["gefa"]) == 1 and t["gefa"][0] > 0 and t["gesl"][0] > 0
+    assert np.all(np.abs(b_dev - 1.0) < 1e-3)
+    residn, _ = oracle.residn(b_dev, normb)
+    assert residn < 1.0
+    want = oracle.gefa_nopvt(A)
+    assert np.abs(A_dev - want).max() < 1e-3
+    rel = np.abs(A_dev.astype(np.float64) - want) / np.maximum(1.0, np.abs(want))
+    assert rel.max() < 256 * FLT_EPS
+    # The FP32 solution is as accurate as the reference's own FP32 solution.
+    x_ref = oracle.gesl_nopvt(want, b)
+    assert np.abs(b_dev - 1.0).max() <= 4 * max(np.abs(x_ref - 1.0).max(), n * FLT_EPS)
+
+
+def test_calculate_repetitions_restart_from_original(ctx):
+    n, bs = 256, 64
+    A, b, _, _ = oracle.gen_reference(n)
+    A1, b1 = A.copy(), b.copy()
+    t = ctx.calculate(A1, b1, bs, repetitions=3)
+    assert len(t["gefa"]) == 3 and len(t["gesl"]) == 3
+    A2, b2 = A.copy(), b.copy()
+    ctx.calculate(A2, b2, bs, repetitions=1)
+    assert np.array_equal(A1, A2) and np.array_equal(b1, b2)
+
+
+@pytest.mark.parametrize("n,bs", [(1024, 128), (2048, 512)])
+def test_baseline_inputs_hpl_residual(ctx, n, bs):
+    """Benchmark generator (seed 42, margin 1): HPL scaled residual with the
+    FP32 unit roundoff <= 16, and FP64-oracle error (x_true = ones exactly)."""
+    A, b64, b32 = oracle.gen_baseline(n, seed=42, margin=1.0)
+    A_dev, x = A.copy(), b32.copy()
+    ctx.calculate(A_dev, x, bs)
+    r = oracle.hpl_resid(A, x.astype(np.float64), b32.astype(np.float64), eps=FLT_EPS / 2)
+    assert r <= 16.0
+    x_cpu = oracle.gesl_nopvt(oracle.gefa_nopvt(A), b32)
+    assert np.abs(x - 1.0).max() <= 4 * np.abs(x_cpu - 1.0).max() + 1e-6
+
+
+@pytest.mark.parametrize("nrhs", [1, 3, 16, 17])
+def test_gesl_multi_rhs(ctx, dev, nrhs):
+    n, bs = 384, 128
+    A, _, _, _ = oracle.gen_reference(n)
+    LU = oracle.gefa_nopvt(A)
+    rng = np.random.default_rng(nrhs)
+    B = rng.uniform(-1, 1, (nrhs, n)).astype(np.float32)
+    dLU, dB = dev.put(LU), dev.put(B)
+    ctx.gesl(dLU.data_ptr(), n, n, dB.data_ptr(), nrhs, n)
+    X = dev.get(dB)
+    LU64 = LU.astype(np.float64)
+    for r in range(nrhs):
+        x64 = oracle.gesl_nopvt(LU64, B[r].astype(np.float64))
+        x32 = oracle.gesl_nopvt(LU, B[r])
+        tol = 8 * np.abs(x32 - x64).max() + 64 * FLT_EPS * np.abs(x64).max()
+        assert np.abs(X[r] - x64).max() <= tol
+
+
+def test_gefa_dev_deterministic(ctx, dev):
+    n, bs = 1024, 256
+    A, _, _, _ = oracle.gen_reference(n)
+    d1, d2 = dev.put(A), dev.put(A)
+    ctx.gefa(d1.data_ptr(), n, n, bs)
+    ctx.gefa(d2.data_ptr(), n, n, bs)
+    assert np.array_equal(dev.get(d1), dev.get(d2))
+
+
+def test_solve_host_f32_and_refined(ctx):
+    n, bs = 1024, 128
+    A, b64, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
+    x, t = ctx.solve_host(A, b64, bs, "f32", max_iters=0)
+    assert t["ir_iters"] == 0
+    r32 = oracle.hpl_resid(A, x, b64, eps=FLT_EPS / 2)
+    assert r32 <= 16.0
+    assert np.isclose(t["hpl_resid"], oracle.hpl_resid(A, x, b64), rtol=1e-6)
+    x2, t2 = ctx.solve_host(A, b64, bs, "f32", max_iters=10)
+    assert t2["hpl_resid"] <= 16.0 and t2["ir_iters"] >= 1
+    assert oracle.hpl_resid(A, x2, b64) <= 16.0
+    # Refinement stops at the HPL threshold, not at full FP64 accuracy.
+    assert np.abs(x2 - 1.0).max() < 1e-10
+
+
+def test_non_dominant_matrix_reports_numeric_error(ctx, lp):
+    """A zero pivot (not factorable without pivoting) must surface as
+    LP_E_NUMERIC, not as a silent result."""
+    n, bs = 128, 64
+    A = np.zeros((n, n), np.float32)
+    A[0, 1] = 1.0
+    with pytest.raises(lp.LpError) as e:
+        ctx.solve_host(A, np.ones(n), bs, "f32")
+    assert e.value.status == lp.LP_E_NUMERIC
+
+
+def test_bad_sizes_rejected(ctx, lp):
+    A = np.zeros((100, 100), np.float32)
+    with pytest.raises(lp.LpError) as e:
+        ctx.calculate(A, np.zeros(100, np.float32), 64)
+    assert e.value.status == lp.LP_E_INVALID
