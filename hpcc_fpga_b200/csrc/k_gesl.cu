@@ -21,16 +21,95 @@ namespace {
 
 constexpr int SB = 128;
 constexpr int GT = 256;            // threads per CTA
-constexpr int GCOLS = GT;          // columns per CTA in step (b)
+constexpr int GCOLS = 128;         // columns per CTA in step (b)
 
 __device__ __forceinline__ float pick4(const float (&y)[4], int q) {
     return q == 0 ? y[0] : (q == 1 ? y[1] : (q == 2 ? y[2] : y[3]));
 }
 
+// Step (b): w[r][c] += sum_{k<kb} coef[r][k] * a[(k0+k)*lda + c] for the
+// CTA's 128 columns c in [col0, colend).  Warp w takes rows 16w..16w+15 of
+// the block, each lane 4 adjacent columns (16-byte loads, 16 independent
+// loads in flight per thread); the 8 warps' partial sums meet in shared
+// memory (`red`, 8 x NR x 128 floats, the diagonal block's buffer reused).
+template <int NR>
+__device__ __forceinline__ void panel_gemv(const float* __restrict__ a, int lda, int k0, int kb, int col0,
+                                           int colend, const float* coef, float* red, float* __restrict__ w,
+                                           int ldw, int nrhs) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c = col0 + lane * 4;
+    float acc[NR][4];
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[r][j] = 0.0f;
+    const int kbeg = warp * 16;
+    if (c + 3 < colend) {
+#pragma unroll
+        for (int kk = 0; kk < 16; kk++) {
+            const int k = kbeg + kk;
+            if (k < kb) {
+                const float4 v = *reinterpret_cast<const float4*>(a + (size_t)(k0 + k) * lda + c);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    const float s = coef[r * SB + k];
+                    acc[r][0] = fmaf(s, v.x, acc[r][0]);
+                    acc[r][1] = fmaf(s, v.y, acc[r][1]);
+                    acc[r][2] = fmaf(s, v.z, acc[r][2]);
+                    acc[r][3] = fmaf(s, v.w, acc[r][3]);
+                }
+            }
+        }
+    } else if (c < colend) {
+        for (int kk = 0; kk < 16; kk++) {
+            const int k = kbeg + kk;
+            if (k >= kb) break;
+            const float* row = a + (size_t)(k0 + k) * lda + c;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+                if (c + j < colend) {
+                    const float v = row[j];
+#pragma unroll
+                    for (int r = 0; r < NR; r++) acc[r][j] = fmaf(coef[r * SB + k], v, acc[r][j]);
+                }
+        }
+    }
+    __syncthreads();  // the caller's use of `red` (the diagonal block) is over
+#pragma unroll
+    for (int r = 0; r < NR; r++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) red[(warp * NR + r) * GCOLS + lane * 4 + j] = acc[r][j];
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < NR * GCOLS; idx += GT) {
+        const int r = idx / GCOLS, cc = idx - r * GCOLS;
+        if (r < nrhs && col0 + cc < colend) {
+            float s = 0.0f;
+#pragma unroll
+            for (int q = 0; q < GT / 32; q++) s += red[(q * NR + r) * GCOLS + cc];
+            w[(size_t)r * ldw + col0 + cc] += s;
+        }
+    }
+}
+
+// The kb x kb diagonal block into shared memory (row length SB): 16-byte
+// loads, all of a thread's 16 loads issued before any is consumed.
 __device__ __forceinline__ void stage_diag(float* dg, const float* __restrict__ a, int lda, int k0, int kb) {
-    for (int idx = threadIdx.x; idx < kb * SB; idx += GT) {
-        const int r = idx >> 7, c = idx & (SB - 1);
-        dg[idx] = (c < kb) ? a[(size_t)(k0 + r) * lda + k0 + c] : 0.0f;
+#pragma unroll
+    for (int it = 0; it < SB * SB / 4 / GT; it++) {
+        const int idx = threadIdx.x + it * GT;
+        const int r = idx >> 5, c = (idx & 31) * 4;
+        float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (r < kb) {
+            const float* src = a + (size_t)(k0 + r) * lda + k0 + c;
+            if (c + 3 < kb) {
+                v = *reinterpret_cast<const float4*>(src);
+            } else {
+                if (c < kb) v.x = src[0];
+                if (c + 1 < kb) v.y = src[1];
+                if (c + 2 < kb) v.z = src[2];
+            }
+        }
+        *reinterpret_cast<float4*>(dg + r * SB + c) = v;
     }
 }
 
@@ -71,22 +150,8 @@ __global__ void __launch_bounds__(GT) k_gesl_fwd(const float* __restrict__ a, in
         }
     }
     __syncthreads();
-    const int i = k0 + kb + blockIdx.x * GCOLS + threadIdx.x;
-    if (i < n) {
-        float acc[NR];
-#pragma unroll
-        for (int r = 0; r < NR; r++) acc[r] = 0.0f;
-        const float* col = a + (size_t)k0 * lda + i;
-#pragma unroll 4
-        for (int k = 0; k < kb; k++) {
-            const float v = col[(size_t)k * lda];
-#pragma unroll
-            for (int r = 0; r < NR; r++) acc[r] = fmaf(ys[r * SB + k], v, acc[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < NR; r++)
-            if (r < nrhs) w1[(size_t)r * ldw + i] += acc[r];
-    }
+    const int col0 = k0 + kb + blockIdx.x * GCOLS;
+    if (col0 < n) panel_gemv<NR>(a, lda, k0, kb, col0, n, ys, dg, w1, ldw, nrhs);
 }
 
 template <int NR>
@@ -133,22 +198,8 @@ __global__ void __launch_bounds__(GT) k_gesl_bwd(const float* __restrict__ a, in
         }
     }
     __syncthreads();
-    const int i = blockIdx.x * GCOLS + threadIdx.x;
-    if (i < k0) {
-        float acc[NR];
-#pragma unroll
-        for (int r = 0; r < NR; r++) acc[r] = 0.0f;
-        const float* col = a + (size_t)k0 * lda + i;
-#pragma unroll 4
-        for (int k = 0; k < kb; k++) {
-            const float v = col[(size_t)k * lda];
-#pragma unroll
-            for (int r = 0; r < NR; r++) acc[r] = fmaf(ss[r * SB + k], v, acc[r]);
-        }
-#pragma unroll
-        for (int r = 0; r < NR; r++)
-            if (r < nrhs) w2[(size_t)r * ldw + i] += acc[r];
-    }
+    const int col0 = blockIdx.x * GCOLS;
+    if (col0 < k0) panel_gemv<NR>(a, lda, k0, kb, col0, k0, ss, dg, w2, ldw, nrhs);
 }
 
 template <int NR>

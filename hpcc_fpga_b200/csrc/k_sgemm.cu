@@ -1,14 +1,17 @@
-// inner stage, FP32: the trailing update of one block step as ONE launch over
+// inner stage, FP32: C(m x n) += At^T * B on k-major operands
+// (At: k x m, B: k x n, rows of contiguous floats).
+//
+// The trailing update of one block step runs as one or a few launches over
 // the whole trailing matrix (the reference issues one inner_update_mm task
 // per b x b block, hpl_torus_PCIE.cl:711-865, execution_pcie.hpp:523-583):
+// C += L * T with L given transposed.  The blocked top/left stages use the
+// same kernel for their chunk-to-rest updates.
 //
-//     C(m x n) += L(m x k) * T(k x n),   L given transposed (Lt, k x m).
-//
-// Both operands are k-major rows of contiguous floats, so every tile load is
-// a run of 16-byte cp.async copies into a STAGES-deep shared-memory ring.
-// 128 x 128 x 16 tiles, 256 threads, 8 x 8 FP32 accumulators per thread
-// (two 4-row and two 4-column groups, conflict-free float4 shared loads),
-// FFMA on the FP32 pipe.  C is read and written once per launch.
+// Both operands are k-major, so every tile load is a run of 16-byte cp.async
+// copies into a STAGES-deep shared-memory ring.  128 x 128 x 16 tiles, 256
+// threads, 8 x 8 FP32 accumulators per thread (two 4-row and two 4-column
+// groups, conflict-free float4 shared loads), FFMA on the FP32 pipe.  C is
+// read and written once per launch.
 #include "lp_common.cuh"
 
 namespace lp {

@@ -129,29 +129,114 @@ static int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
     return LP_OK;
 }
 
+// top stage for a whole block row: T (bs x ncols) <- top recurrence with the
+// factored diagonal block d.  bs <= 128: one exact-recurrence launch.  Larger
+// blocks walk 128-row diagonal chunks: exact recurrence on the chunk's rows
+// (full width, every column strip in parallel), then the chunk's
+// contribution to the rows below as one GEMM, T[below] += D[below][chunk] *
+// T[chunk] (D's sub-block transposed into the k-major operand first).
+static int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols,
+                       cudaStream_t st) {
+    if (bs <= 128) return launch_trsm_top(d, lda, t, ldt, bs, ncols, st);
+    const int ib = 128;
+    float* dt = static_cast<float*>(c->dsub.ptr) + (st == c->aux ? (size_t)ib * bs : 0);
+    for (int kk = 0; kk < bs / ib; kk++) {
+        const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        float* tk = t + (size_t)kk * ib * ldt;
+        LP_CHECK(launch_trsm_top(dkk, lda, tk, ldt, ib, ncols, st));
+        const int m2 = bs - (kk + 1) * ib;
+        if (m2 <= 0) break;
+        LP_CHECK(launch_transpose(dkk + (size_t)ib * lda, lda, dt, m2, m2, ib, st));
+        LP_CHECK(launch_sgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, ncols, ib, st));
+    }
+    return LP_OK;
+}
+
+// left stage for a whole block column: L (nrows x bs) <- left recurrence with
+// d, and Lt = L^T.  Larger blocks walk 128-column chunks: exact recurrence on
+// the chunk's columns (which also writes the chunk's rows of Lt), then
+// L[:, after] += L[:, chunk] * D[chunk][after] as one GEMM.
+static int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
+                        cudaStream_t st) {
+    if (bs <= 128) return launch_trsm_left(d, lda, l, ldl, bs, nrows, lt, ldlt, st);
+    const int ib = 128;
+    for (int kk = 0; kk < bs / ib; kk++) {
+        const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        float* lk = l + (size_t)kk * ib;
+        float* ltk = lt + (size_t)kk * ib * ldlt;
+        LP_CHECK(launch_trsm_left(dkk, lda, lk, ldl, ib, nrows, ltk, ldlt, st));
+        const int m2 = bs - (kk + 1) * ib;
+        if (m2 <= 0) break;
+        LP_CHECK(launch_sgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, nrows, m2, ib, st));
+    }
+    return LP_OK;
+}
+
+// Panel work of block step K: lu on the diagonal block, then the top block
+// row and the left block column (Lt written into `lt`).
+static int panel(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st) {
+    float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+    const double b = bs;
+    int e = prof_begin(c, st);
+    LP_CHECK(lu_stage(c, d, lda, bs, st));
+    LP_CHECK(prof_end(c, st, LP_STAGE_LU, e, lu_flops(b), 8.0 * b * b));
+    const int rest = n - (K + 1) * bs;
+    if (rest <= 0) return LP_OK;
+    const double r = rest;
+    e = prof_begin(c, st);
+    LP_CHECK(top_blocked(c, d, lda, d + bs, lda, bs, rest, st));
+    LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, trsm_flops(b, r), 8.0 * b * r));
+    e = prof_begin(c, st);
+    LP_CHECK(left_blocked(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
+    LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
+    return LP_OK;
+}
+
+// Blocked right-looking LU without pivoting (the block-row loop of
+// execution_pcie.hpp:177-641, on one GPU) with one step of look-ahead.
+// Step K's trailing update C += L_K * T_K is split: first the next block row
+// and block column (U_a), then the rest (U_b).  As soon as U_a is done the
+// panel of step K+1 (lu, top, left) runs on the high-priority auxiliary
+// stream while U_b runs on the main stream; they touch disjoint blocks, and
+// Lt is double-buffered so panel K+1 never overwrites the operand U_b reads.
+// top and left give the reference recurrences' values up to rounding
+// (blocked); the exact recurrences are lp_top_update_dev/lp_left_update_dev.
 int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
-    LP_CHECK(c->lt.ensure(sizeof(float) * (size_t)bs * n));
-    if (bs > 128) LP_CHECK(c->lti.ensure(sizeof(float) * (size_t)128 * bs));
-    float* lt = static_cast<float*>(c->lt.ptr);
+    const size_t pan = sizeof(float) * (size_t)bs * n;
+    LP_CHECK(c->lt.ensure(2 * pan));
+    if (bs > 128) {
+        LP_CHECK(c->lti.ensure(2 * sizeof(float) * (size_t)128 * bs));
+        LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
+    }
+    float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + (size_t)bs * n};
     const int nb = n / bs;
     const double b = bs;
-    for (int K = 0; K < nb; K++) {
-        float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
-        int e = prof_begin(c, st);
-        LP_CHECK(lu_stage(c, d, lda, bs, st));
-        LP_CHECK(prof_end(c, st, LP_STAGE_LU, e, lu_flops(b), 8.0 * b * b));
+    LP_CHECK(panel(c, dA, n, lda, bs, 0, ltbuf[0], st));
+    for (int K = 0; K + 1 < nb; K++) {
         const int rest = n - (K + 1) * bs;
-        if (rest <= 0) break;
         const double r = rest;
-        e = prof_begin(c, st);
-        LP_CHECK(launch_trsm_top(d, lda, d + bs, lda, bs, rest, st));
-        LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, trsm_flops(b, r), 8.0 * b * r));
-        e = prof_begin(c, st);
-        LP_CHECK(launch_trsm_left(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
-        LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
-        e = prof_begin(c, st);
-        LP_CHECK(launch_sgemm_update(d + (size_t)bs * lda + bs, lda, lt, rest, d + bs, lda, rest, rest, bs, st));
-        LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(r, r, b), inner_bytes(r, r, b)));
+        float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+        float* top = d + bs;
+        float* lt = ltbuf[K & 1];
+        float* c11 = d + (size_t)bs * lda + bs;
+        int e = prof_begin(c, st);
+        LP_CHECK(launch_sgemm_update(c11, lda, lt, rest, top, lda, bs, rest, bs, st));
+        if (rest > bs)
+            LP_CHECK(launch_sgemm_update(c11 + (size_t)bs * lda, lda, lt + bs, rest, top, lda, rest - bs, bs, bs, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(b, r, b) + inner_flops(r - b, b, b),
+                          inner_bytes(b, r, b) + inner_bytes(r - b, b, b)));
+        LP_CUDA(cudaEventRecord(c->ev_fork, st));
+        LP_CUDA(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
+        LP_CHECK(panel(c, dA, n, lda, bs, K + 1, ltbuf[(K + 1) & 1], c->aux));
+        LP_CUDA(cudaEventRecord(c->ev_join, c->aux));
+        if (rest > bs) {
+            const double r2 = rest - bs;
+            e = prof_begin(c, st);
+            LP_CHECK(launch_sgemm_update(c11 + (size_t)bs * lda + bs, lda, lt + bs, rest, top + bs, lda, rest - bs,
+                                         rest - bs, bs, st));
+            LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(r2, r2, b), inner_bytes(r2, r2, b)));
+        }
+        LP_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));
     }
     return LP_OK;
 }
@@ -228,7 +313,12 @@ int lp_ctx_create(int device, lp_ctx** out) {
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
     std::snprintf(c->name, sizeof(c->name), "%s", prop.name);
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->aux, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         lp_ctx_destroy(c);
@@ -242,9 +332,13 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c == nullptr) return LP_OK;
     cudaSetDevice(c->device);
     if (c->stream != nullptr) cudaStreamSynchronize(c->stream);
+    if (c->aux != nullptr) cudaStreamSynchronize(c->aux);
     c->release_all();
     for (int i = 0; i < 8; i++)
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
+    if (c->ev_fork != nullptr) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join != nullptr) cudaEventDestroy(c->ev_join);
+    if (c->aux != nullptr) cudaStreamDestroy(c->aux);
     if (c->stream != nullptr) cudaStreamDestroy(c->stream);
     delete c;
     return LP_OK;
@@ -353,6 +447,8 @@ int lp_gefa_dev(lp_ctx* c, float* dA, int n, int lda, int bs) {
 int lp_gesl_dev(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb) {
     if (c == nullptr || dLU == nullptr || dB == nullptr) return fail(LP_E_INVALID, "lp_gesl_dev: null argument");
     if (n <= 0 || lda < n || nrhs <= 0 || ldb < n) return fail(LP_E_INVALID, "lp_gesl_dev: bad sizes");
+    if (lda % 4 != 0 || !aligned16(dLU))
+        return fail(LP_E_INVALID, "lp_gesl_dev: factors must be 16-byte aligned with lda a multiple of 4");
     LP_CUDA(cudaSetDevice(c->device));
     return gesl_f32(c, dLU, n, lda, dB, nrhs, ldb, c->stream);
 }

@@ -43,6 +43,7 @@ int launch_trsm_left(const float* lu, int ldlu, float* l, int ldl, int bs, int n
 // FP32 SIMT trailing update C(m x n) += Lt^T (bs x m) * T (bs x n).
 int launch_sgemm_update(float* c, int ldc, const float* lt, int ldlt, const float* t, int ldt, int m, int n,
                         int k, cudaStream_t s);
+int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t s);
 // Forward + back substitution for nrhs rows of b (see k_gesl.cu).
 int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t s);
 size_t gesl_work_floats(int n, int nrhs);

@@ -40,9 +40,12 @@ struct lp_ctx {
     int num_sms = 0;
     char name[256] = {0};
     cudaStream_t stream = nullptr;
+    cudaStream_t aux = nullptr;               // second (high-priority) stream for concurrent panel work
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev[8] = {nullptr};
-    lp::Workspace lt;    // transposed left panel (bs x n)
-    lp::Workspace lti;   // transposed inner left panel of the recursive lu stage
+    lp::Workspace lt;    // transposed left panels (2 x bs x n, alternating by block step)
+    lp::Workspace dsub;  // transposed diagonal sub-blocks of the blocked top stage (per stream)
+    lp::Workspace lti;   // transposed inner left panel of the recursive lu stage (per stream)
     lp::Workspace gw;    // substitution work vectors
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
@@ -53,7 +56,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &lti, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
         for (auto* w : all) w->release();
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();
