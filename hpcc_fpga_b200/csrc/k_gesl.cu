@@ -14,6 +14,8 @@
 //       each factor element read once per sweep, for all right-hand sides).
 // The accumulating vector and the solved vector are separate buffers, so
 // step (a) of launch K never reads what step (b) of launch K writes.
+#include <mutex>
+
 #include "lp_common.cuh"
 
 namespace lp {
@@ -249,6 +251,35 @@ size_t gesl_work_floats(int n, int nrhs) {
     return 2 * (size_t)n * (size_t)g;
 }
 
+// ---- allocation-free variant (lp_gesl_dev_noalloc) ---------------------------
+// Its two work vectors live in this fixed device array instead of a context
+// workspace: 2^20 floats (4 MiB), enough for 2 * n * min(nrhs, 16) <= 2^20.
+// Every GPU that loads the library holds the array until the process exits.
+// Host code only sees a host-side stand-in for the array's name; the device
+// address is looked up once per device with cudaGetSymbolAddress.
+constexpr size_t kNoAllocScratchFloats = size_t(1) << 20;
+static __device__ __align__(256) float g_gesl_scratch[kNoAllocScratchFloats];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {nullptr};
+
+// Once per device, with that device current: attributes of the substitution
+// kernels and the scratch array's device address.
+int noalloc_setup(int dev, float** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        LP_CHECK(gesl_init_attrs());
+        void* p = nullptr;
+        LP_CUDA(cudaGetSymbolAddress(&p, g_gesl_scratch));
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return LP_OK;
+}
+}  // namespace
+
 int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return LP_OK;
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
@@ -269,3 +300,20 @@ int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, flo
 }
 
 }  // namespace lp
+
+extern "C" int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, void* stream) {
+    using namespace lp;
+    if (dLU == nullptr || dB == nullptr) return fail(LP_E_INVALID, "lp_gesl_dev_noalloc: null argument");
+    if (n <= 0 || lda < n || nrhs <= 0 || ldb < n) return fail(LP_E_INVALID, "lp_gesl_dev_noalloc: bad sizes");
+    if (lda % 4 != 0 || !aligned16(dLU))
+        return fail(LP_E_INVALID, "lp_gesl_dev_noalloc: factors must be 16-byte aligned with lda a multiple of 4");
+    if (gesl_work_floats(n, nrhs) > kNoAllocScratchFloats)
+        return fail(LP_E_INVALID, "lp_gesl_dev_noalloc: 2 * n * min(nrhs, 16) exceeds the fixed scratch of 1048576 "
+                                  "floats (4 MiB); use lp_gesl_dev for larger systems");
+    int dev = 0;
+    LP_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return fail(LP_E_INVALID, "lp_gesl_dev_noalloc: device index out of range");
+    float* scratch = nullptr;
+    LP_CHECK(noalloc_setup(dev, &scratch));
+    return launch_gesl(dLU, lda, n, dB, ldb, nrhs, scratch, static_cast<cudaStream_t>(stream));
+}

@@ -96,6 +96,7 @@ def lib() -> ctypes.CDLL:
     L.lp_inner_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _VP, _I, _I, _I, _I]
     L.lp_gefa_dev.argtypes = [_VP, _VP, _I, _I, _I]
     L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
+    L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
     L.lp_solve_host.argtypes = [_VP, _I, _I, _I, _F32P, _I, _F64P, _I, _F64P, _I, ctypes.POINTER(LpTiming)]
     L.lp_generate_reference.argtypes = [_F32P, _F32P, _I, _I, ctypes.POINTER(ctypes.c_float),

@@ -145,6 +145,24 @@ int lp_gefa_dev(lp_ctx* ctx, float* dA, int n, int lda, int bs);
  * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229). */
 int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb);
 
+/* The same substitution for callers that cannot allocate device memory: no
+ * counterpart in the reference.  Some callers must not call cudaMalloc or
+ * cudaFree — code that hands all device memory to its own pool, code that
+ * records CUDA graphs or runs inside a latency-bound serving loop (where an
+ * allocation can synchronize the device), or a plugin host that forbids it.
+ * This entry point allocates nothing and needs no lp_ctx: its two work vectors
+ * live in one fixed device array of 2^20 floats (4 MiB) that every GPU which
+ * loads the library holds until the process exits, so it accepts only
+ * 2 * n * min(nrhs, 16) <= 1048576 and returns LP_E_INVALID beyond that.
+ * The first call on a device (the current device) looks up the array's
+ * address and sets kernel attributes for that device; make that first call
+ * before any stream capture.  All calls share the array and each call fully
+ * rewrites what it reads, but calls whose work overlaps on the GPU (other
+ * streams, other threads, same device) race on it: serialize them.
+ * stream: a cudaStream_t, or NULL for the default stream.  dLU, dB as for
+ * lp_gesl_dev; the solutions overwrite dB. */
+int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, void* stream);
+
 /* ---- host entry points --------------------------------------------------- */
 /* The CUDA execution backend: the drop-in for
  *   std::map<std::string, std::vector<double>> execution::pcie::calculate(
