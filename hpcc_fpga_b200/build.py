@@ -82,7 +82,7 @@ def build(force: bool = False, jobs: int = 8, verbose: bool = False) -> str:
         objs = [f.result() for f in futs]
     so = os.path.join(LIB, SONAME)
     if force or _stale(so, objs):
-        _run([nvcc_path(), *ARCH, "-shared", "-o", so, *objs, "-lcuda"])
+        _run([nvcc_path(), *ARCH, "-shared", "-o", so, *objs])
         if verbose:
             print("linked", so)
     harness = build_harness(force)

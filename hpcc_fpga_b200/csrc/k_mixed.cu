@@ -1,11 +1,218 @@
-// Mixed-precision factorization (tensor-core trailing update): see gefa_mixed.
+// Mixed-precision factorization: the block schedule of gefa_f32 (lu, top,
+// left in FP32, one step of look-ahead) with the trailing update on the
+// tensor cores (k_umma.cu).  After each panel its left block column L and top
+// block row T are rounded to the tensor-core operand type:
+//   BF16:  Lq[m][k] = bf16(L[m][k]),  Tq[n][k] = bf16(T[k][n]);
+//   E4M3:  one absmax scale per 512-row block of L and per 512-column block
+//          of T (s = absmax / 448), Lq = e4m3(L / s_L), Tq = e4m3(T^T / s_T),
+//          and the update adds s_L * s_T * (Lq Tq^T) in FP32.
+// The FP32 factors the substitution uses are these rounded-update factors;
+// accuracy is recovered by FP64 iterative refinement (lp_solve.cu).
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
 #include "lp_ctx.cuh"
 
 namespace lp {
+namespace {
+
+constexpr float kE4M3Max = 448.0f;
+
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+    atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));  // non-negative floats order as ints
+}
+
+// amax[r / 512] = max |L[r][0..k)| over each 512-row block.
+__global__ void k_absmax_rows(const float* __restrict__ L, int ldl, int rows, int k, float* __restrict__ amax) {
+    const int r = blockIdx.x;
+    float m = 0.0f;
+    for (int c = threadIdx.x; c < k; c += blockDim.x) m = fmaxf(m, fabsf(L[(size_t)r * ldl + c]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&amax[r >> 9], m);
+}
+
+// amax[c / 512] = max |T[0..k)[c]| over each 512-column block.
+__global__ void k_absmax_cols(const float* __restrict__ T, int ldt, int k, int cols, float* __restrict__ amax) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float m = 0.0f;
+    for (int r = 0; r < k; r++) m = fmaxf(m, fabsf(T[(size_t)r * ldt + c]));
+    atomic_max_nonneg(&amax[c >> 9], m);
+}
+
+// scale = amax / 448 (1 for an all-zero block); inv = 1 / scale.
+__global__ void k_scales(const float* __restrict__ amax, float* __restrict__ scale, float* __restrict__ inv, int nb) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    const float a = amax[i];
+    const float s = a > 0.0f ? a / kE4M3Max : 1.0f;
+    scale[i] = s;
+    inv[i] = 1.0f / s;
+}
+
+template <bool FP8>
+__global__ void k_quant_rows(const float* __restrict__ L, int ldl, uint8_t* __restrict__ out, int rows, int k,
+                             const float* __restrict__ inv) {
+    const size_t total = (size_t)rows * k / 4;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const size_t e = i * 4;
+        const int r = (int)(e / k), c = (int)(e - (size_t)r * k);
+        float4 v = *reinterpret_cast<const float4*>(L + (size_t)r * ldl + c);
+        if (FP8) {
+            const float s = inv[r >> 9];
+            __nv_fp8x4_e4m3 q(make_float4(v.x * s, v.y * s, v.z * s, v.w * s));
+            *reinterpret_cast<__nv_fp8x4_e4m3*>(out + e) = q;
+        } else {
+            __nv_bfloat162 lo = __floats2bfloat162_rn(v.x, v.y), hi = __floats2bfloat162_rn(v.z, v.w);
+            __nv_bfloat162* o = reinterpret_cast<__nv_bfloat162*>(out + e * 2);
+            o[0] = lo;
+            o[1] = hi;
+        }
+    }
+}
+
+// out[c][r] = q(T[r][c]) for r < k, c < cols: 32 x 32 tiles through shared memory.
+template <bool FP8>
+__global__ void __launch_bounds__(256) k_quant_trans(const float* __restrict__ T, int ldt, uint8_t* __restrict__ out,
+                                                     int k, int cols, const float* __restrict__ inv) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int r = r0 + ty + j, c = c0 + tx;
+        tile[ty + j][tx] = (r < k && c < cols) ? T[(size_t)r * ldt + c] : 0.0f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int c = c0 + ty + j, r = r0 + tx;
+        if (r < k && c < cols) {
+            const float v = tile[tx][ty + j];
+            if (FP8) {
+                __nv_fp8_e4m3 q(v * inv[c >> 9]);
+                out[(size_t)c * k + r] = *reinterpret_cast<uint8_t*>(&q);
+            } else {
+                __nv_bfloat16 q = __float2bfloat16_rn(v);
+                reinterpret_cast<__nv_bfloat16*>(out)[(size_t)c * k + r] = q;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// Rounds the panel of a block step to the tensor-core operand type.
+// L: rows_l x k (ld ldl), T: k x cols_t (ld ldt); aq: rows_l x k, bq:
+// cols_t x k; sc: 3 arrays of nblk floats (absmax, scale, 1/scale) for L,
+// then 3 for T (nblk >= ceil(max(rows_l, cols_t) / 512)).
+int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
+                   uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st) {
+    if (rows_l <= 0 || cols_t <= 0) return LP_OK;
+    const size_t q4 = (size_t)rows_l * k / 4;
+    const int qgrid = (int)((q4 + 255) / 256 < 2368 ? (q4 + 255) / 256 : 2368);
+    const dim3 tgrid((cols_t + 31) / 32, (k + 31) / 32);
+    if (fp8) {
+        float* amax_a = sc;
+        float* scale_a = sc + nblk;
+        float* inv_a = sc + 2 * nblk;
+        float* amax_b = sc + 3 * nblk;
+        float* scale_b = sc + 4 * nblk;
+        float* inv_b = sc + 5 * nblk;
+        LP_CUDA(cudaMemsetAsync(amax_a, 0, sizeof(float) * nblk, st));
+        LP_CUDA(cudaMemsetAsync(amax_b, 0, sizeof(float) * nblk, st));
+        k_absmax_rows<<<rows_l, 128, 0, st>>>(L, ldl, rows_l, k, amax_a);
+        k_absmax_cols<<<(cols_t + 255) / 256, 256, 0, st>>>(T, ldt, k, cols_t, amax_b);
+        k_scales<<<(nblk + 127) / 128, 128, 0, st>>>(amax_a, scale_a, inv_a, nblk);
+        k_scales<<<(nblk + 127) / 128, 128, 0, st>>>(amax_b, scale_b, inv_b, nblk);
+        k_quant_rows<true><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, inv_a);
+        k_quant_trans<true><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, inv_b);
+        count_launch(6);
+    } else {
+        k_quant_rows<false><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, nullptr);
+        k_quant_trans<false><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, nullptr);
+        count_launch(2);
+    }
+    LP_CUDA(cudaGetLastError());
+    return LP_OK;
+}
+
+// One trailing (sub)update of the mixed schedule: rows [m_off, m_off+m) and
+// columns [n_off, n_off+n) of the trailing matrix at c11.
+static int mixed_update(lp_ctx* c, float* c11, int lda, const uint8_t* aq, const uint8_t* bq, int rest, int m_off,
+                        int n_off, int m, int n, int bs, bool fp8, const float* sc, int nblk, cudaStream_t st) {
+    const float* scale_a = fp8 ? sc + nblk : nullptr;
+    const float* scale_b = fp8 ? sc + 4 * nblk : nullptr;
+    return launch_umma_update(c11, lda, aq, rest, bq, rest, m_off, n_off, m, n, bs, fp8, scale_a, scale_b,
+                              static_cast<int*>(c->err.ptr), st);
+}
 
 int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st) {
-    (void)c; (void)precision; (void)dA; (void)n; (void)lda; (void)bs; (void)st;
-    return fail(LP_E_INVALID, "mixed-precision factorization is not available in this build");
+    const bool fp8 = precision == LP_FP8_IR;
+    if (bs < 128 || bs % 128 != 0) return fail(LP_E_INVALID, "mixed precision needs a block size >= 128");
+    const size_t esz = fp8 ? 1 : 2;
+    const size_t pan = (size_t)bs * n;
+    const int nblk = (n + 511) / 512;
+    LP_CHECK(c->lt.ensure(2 * sizeof(float) * pan));
+    if (bs > 128) {
+        LP_CHECK(c->lti.ensure(2 * sizeof(float) * (size_t)128 * bs));
+        LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
+    }
+    LP_CHECK(c->q.ensure(4 * esz * pan));
+    LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)nblk));
+    LP_CHECK(c->err.ensure(sizeof(int)));
+    LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
+    float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + pan};
+    uint8_t* q = static_cast<uint8_t*>(c->q.ptr);
+    uint8_t* aqb[2] = {q, q + 2 * esz * pan};
+    uint8_t* bqb[2] = {q + esz * pan, q + 3 * esz * pan};
+    float* scb[2] = {static_cast<float*>(c->qs.ptr), static_cast<float*>(c->qs.ptr) + 6 * nblk};
+    const int nb = n / bs;
+    const double b = bs;
+
+    auto panel_q = [&](int K, cudaStream_t s) -> int {
+        LP_CHECK(panel_f32(c, dA, n, lda, bs, K, ltbuf[K & 1], s));
+        const int rest = n - (K + 1) * bs;
+        if (rest <= 0) return LP_OK;
+        float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+        const int e = prof_begin(c, s);
+        LP_CHECK(quantize_panel(d + (size_t)bs * lda, lda, d + bs, lda, rest, rest, bs, fp8, aqb[K & 1],
+                                bqb[K & 1], scb[K & 1], nblk, s));
+        return prof_end(c, s, LP_STAGE_OTHER, e, 0.0, 2.0 * 4.0 * b * rest + 2.0 * esz * b * rest);
+    };
+
+    LP_CHECK(panel_q(0, st));
+    for (int K = 0; K + 1 < nb; K++) {
+        const int rest = n - (K + 1) * bs;
+        const double r = rest;
+        float* c11 = dA + (size_t)(K + 1) * bs * lda + (size_t)(K + 1) * bs;
+        const uint8_t* aq = aqb[K & 1];
+        const uint8_t* bq = bqb[K & 1];
+        const float* sc = scb[K & 1];
+        int e = prof_begin(c, st);
+        LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, 0, 0, bs, rest, bs, fp8, sc, nblk, st));
+        if (rest > bs) LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, 0, rest - bs, bs, bs, fp8, sc, nblk, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, 2.0 * b * r * b + 2.0 * (r - b) * b * b,
+                          8.0 * (b * r + (r - b) * b)));
+        LP_CUDA(cudaEventRecord(c->ev_fork, st));
+        LP_CUDA(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
+        LP_CHECK(panel_q(K + 1, c->aux));
+        LP_CUDA(cudaEventRecord(c->ev_join, c->aux));
+        if (rest > bs) {
+            const double r2 = rest - bs;
+            e = prof_begin(c, st);
+            LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, bs, rest - bs, rest - bs, bs, fp8, sc, nblk, st));
+            LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, 2.0 * r2 * r2 * b, 8.0 * r2 * r2));
+        }
+        LP_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));
+    }
+    int herr = 0;
+    LP_CUDA(cudaMemcpyAsync(&herr, c->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    if (herr != 0)
+        return fail(LP_E_TIMEOUT, "tensor-core trailing update: a bounded wait expired (code " +
+                                      std::to_string(herr) + "); the update was abandoned");
+    return LP_OK;
 }
 
 }  // namespace lp

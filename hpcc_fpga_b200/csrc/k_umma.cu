@@ -1,0 +1,344 @@
+// inner stage on the 5th-generation tensor cores (mixed-precision form):
+//
+//     C(m x n, FP32) += scale_a[m/512] * scale_b[n/512] * (Aq * Bq^T)
+//
+// Aq: the left panel rounded to BF16 (or FP8 E4M3), m x k, k contiguous;
+// Bq: the top panel rounded the same way and stored transposed, n x k.
+// Both are K-major operands, loaded by TMA with 128-byte swizzle into a
+// STAGES-deep shared-memory ring; one elected thread issues tcgen05.mma
+// (kind::f16 for BF16, kind::f8f6f4 for E4M3) into a 128 x 128 FP32
+// accumulator in tensor memory; after the k loop the four warps read the
+// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile
+// rows) and add it into C, which is read and written once.  The diagonal
+// block and the triangular stages stay FP32 (k_lu.cu, k_trsm.cu).
+//
+// Every mbarrier wait is bounded.  On expiry the thread records an error
+// code in *err, raises the CTA's abort flag, stops issuing work, lets its own
+// copies / MMAs in flight finish (bounded again), and the CTA frees its
+// tensor memory and returns; the host reports LP_E_TIMEOUT.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_fp8.h>
+
+#include "lp_common.cuh"
+
+namespace lp {
+namespace {
+
+constexpr int UM = 128;            // tile rows (TMEM lanes)
+constexpr int UN = 128;            // tile columns (TMEM columns)
+constexpr int UKB = 128;           // bytes of k per stage row (one 128-byte swizzle row)
+constexpr int USTAGES = 3;
+constexpr int UT = 128;            // threads: 4 warps
+constexpr int kTileBytesA = UM * UKB;
+constexpr int kTileBytesB = UN * UKB;
+constexpr int kStageBytes = kTileBytesA + kTileBytesB;
+constexpr size_t kUmmaSmem = (size_t)USTAGES * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
+constexpr uint32_t kSpinLimit = 1u << 26;
+constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;
+
+enum : int { kErrFullWait = 1, kErrEmptyWait = 2, kErrDoneWait = 3 };
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Bounded wait: at most kWaitNs of wall time (and kSpinLimit polls); gives
+// up early when the CTA's abort flag is raised.  Legitimate waits here last
+// microseconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < kSpinLimit; i++) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 63) == 63 && (*abort_flag || global_ns() - t0 > kWaitNs)) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major with 128-byte swizzle: rows of
+// 128 bytes, 8-row core groups 1024 bytes apart (SBO), LBO unused (1),
+// descriptor version 1, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+template <bool FP8>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+    if (FP8) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    }
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Instruction descriptor: FP32 accumulate (c_format 1), A/B K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28; a/b format 1 = BF16 for
+// kind::f16, 0 = E4M3 for kind::f8f6f4.
+template <bool FP8>
+__host__ __device__ constexpr uint32_t idesc_value() {
+    return (1u << 4) | ((FP8 ? 0u : 1u) << 7) | ((FP8 ? 0u : 1u) << 10) | ((uint32_t)(UN >> 3) << 17) |
+           ((uint32_t)(UM >> 4) << 24);
+}
+
+template <bool FP8>
+__global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ CUtensorMap map_a,
+                                                       const __grid_constant__ CUtensorMap map_b,
+                                                       float* __restrict__ C, int ldc, int m_off, int n_off, int kbytes,
+                                                       const float* __restrict__ scale_a,
+                                                       const float* __restrict__ scale_b, int* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* tiles = smem_raw + (base - raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(tiles + USTAGES * kStageBytes);
+    uint64_t* empty = full + USTAGES;
+    uint64_t* done = empty + USTAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = m_off + blockIdx.y * UM;
+    const int n0 = n_off + blockIdx.x * UN;
+    const int KT = kbytes / UKB;
+    constexpr int kSteps = UKB / 32;  // 32 bytes of k per MMA: 16 BF16 or 32 E4M3
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < USTAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)UN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer.
+        int issued = 0;
+        for (int kt = 0; kt < KT; kt++) {
+            const int s = kt % USTAGES;
+            if (!mbar_wait(&empty[s], ((kt / USTAGES) & 1) ^ 1, abort_flag)) {
+                atomicExch(err, kErrEmptyWait);
+                *abort_flag = 1;
+                break;
+            }
+            uint8_t* sa = tiles + s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_2d(sa, &map_a, &full[s], kt * UKB / (FP8 ? 1 : 2), m0);
+            tma_load_2d(sa + kTileBytesA, &map_b, &full[s], kt * UKB / (FP8 ? 1 : 2), n0);
+            issued = kt + 1;
+        }
+        // Let this thread's copies still in flight land before the CTA can exit.
+        for (int kt = issued - USTAGES < 0 ? 0 : issued - USTAGES; kt < issued; kt++) {
+            volatile int no_abort = 0;
+            mbar_wait(&full[kt % USTAGES], (kt / USTAGES) & 1, &no_abort);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer.
+        constexpr uint32_t idesc = idesc_value<FP8>();
+        int kt = 0;
+        for (; kt < KT; kt++) {
+            const int s = kt % USTAGES;
+            if (!mbar_wait(&full[s], (kt / USTAGES) & 1, abort_flag)) {
+                atomicExch(err, kErrFullWait);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t sa = smem_u32(tiles + s * kStageBytes);
+            const uint32_t sb = sa + kTileBytesA;
+#pragma unroll
+            for (int j = 0; j < kSteps; j++)
+                umma<FP8>(tmem, desc_sw128(sa + 32 * j), desc_sw128(sb + 32 * j), idesc, (kt | j) ? 1u : 0u);
+            umma_commit(&empty[s]);
+        }
+        umma_commit(done);  // tracks every MMA issued above, also on the abort path
+    }
+    __syncwarp();
+
+    // Epilogue: all four warps.  Wait for the accumulator (bounded even when
+    // aborting, so no MMA is in flight when tensor memory is freed).
+    {
+        volatile int no_abort = 0;
+        if (!mbar_wait(done, 0, &no_abort)) {
+            if (lane == 0) atomicExch(err, kErrDoneWait);
+            *abort_flag = 1;
+        }
+    }
+    tc_fence_after();
+    if (!*abort_flag) {
+        const float sc = (scale_a != nullptr) ? scale_a[m0 >> 9] * scale_b[n0 >> 9] : 1.0f;
+        const int row = m0 + warp * 32 + lane;
+        float* crow = C + (size_t)row * ldc + n0;
+        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c0 = 0; c0 < UN; c0 += 64) {
+            float4 cv[16];
+#pragma unroll
+            for (int q = 0; q < 16; q++) cv[q] = *reinterpret_cast<const float4*>(crow + c0 + 4 * q);
+            uint32_t r0[32], r1[32];
+            tmem_ld32(tbase + c0, r0);
+            tmem_ld32(tbase + c0 + 32, r1);
+            tmem_wait_ld();
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                cv[q].x = fmaf(sc, __uint_as_float(r0[4 * q + 0]), cv[q].x);
+                cv[q].y = fmaf(sc, __uint_as_float(r0[4 * q + 1]), cv[q].y);
+                cv[q].z = fmaf(sc, __uint_as_float(r0[4 * q + 2]), cv[q].z);
+                cv[q].w = fmaf(sc, __uint_as_float(r0[4 * q + 3]), cv[q].w);
+                cv[q + 8].x = fmaf(sc, __uint_as_float(r1[4 * q + 0]), cv[q + 8].x);
+                cv[q + 8].y = fmaf(sc, __uint_as_float(r1[4 * q + 1]), cv[q + 8].y);
+                cv[q + 8].z = fmaf(sc, __uint_as_float(r1[4 * q + 2]), cv[q + 8].z);
+                cv[q + 8].w = fmaf(sc, __uint_as_float(r1[4 * q + 3]), cv[q + 8].w);
+            }
+#pragma unroll
+            for (int q = 0; q < 16; q++) *reinterpret_cast<float4*>(crow + c0 + 4 * q) = cv[q];
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)UN));
+    }
+}
+
+// ---- host side ---------------------------------------------------------------
+
+// The driver's tensor-map encoder, looked up through the runtime so the
+// library does not link the driver library (it must load on hosts without
+// a GPU driver, where only its host-side entry points are used).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+int encode_fn(EncodeTiledFn* out) {
+    static EncodeTiledFn fn = nullptr;
+    if (fn == nullptr) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        LP_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || p == nullptr)
+            return fail(LP_E_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+        fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    *out = fn;
+    return LP_OK;
+}
+
+// 2-D tensor map over a row-major (rows x kbytes-of-k) operand with 128-byte
+// swizzled boxes of (128 bytes of k) x 128 rows.
+int make_map(CUtensorMap* map, const void* base, int rows, int kelems, bool fp8) {
+    EncodeTiledFn encode = nullptr;
+    LP_CHECK(encode_fn(&encode));
+    const CUtensorMapDataType dt = fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+    const int esz = fp8 ? 1 : 2;
+    const cuuint64_t dims[2] = {(cuuint64_t)kelems, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)kelems * esz};
+    const cuuint32_t box[2] = {(cuuint32_t)(UKB / esz), (cuuint32_t)UM};
+    const cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(LP_E_CUDA, "cuTensorMapEncodeTiled failed: CUresult " + std::to_string((int)r));
+    return LP_OK;
+}
+
+}  // namespace
+
+int umma_init_attrs() {
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem));
+    return LP_OK;
+}
+
+// C(rows m_off..m_off+m, cols n_off..n_off+n of the matrix at c) += scaled
+// product of aq (rows x k, k contiguous) and bq (cols x k).  aq_rows/bq_rows
+// are the operands' full row counts (the tensor-map extents); m, n, m_off,
+// n_off must be multiples of 128; k a multiple of 64 (BF16) / 128 (E4M3).
+int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
+                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
+                       cudaStream_t st) {
+    if (m <= 0 || n <= 0) return LP_OK;
+    const int kbytes = k * (fp8 ? 1 : 2);
+    if (m % UM || n % UN || m_off % UM || n_off % UN || kbytes % UKB || ldc % 4 || !aligned16(c) || !aligned16(aq) ||
+        !aligned16(bq) || m_off + m > aq_rows || n_off + n > bq_rows)
+        return fail(LP_E_INVALID, "umma_update: tile-aligned sizes and 16-byte aligned operands required");
+    if (fp8 && (scale_a == nullptr || scale_b == nullptr)) return fail(LP_E_INVALID, "umma_update: fp8 needs scales");
+    CUtensorMap ma, mb;
+    LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8));
+    LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8));
+    const dim3 grid(n / UN, m / UM);
+    if (fp8)
+        k_umma_update<true><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, kbytes, scale_a, scale_b, err);
+    else
+        k_umma_update<false><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, kbytes, nullptr, nullptr, err);
+    count_launch();
+    LP_CUDA(cudaGetLastError());
+    return LP_OK;
+}
+
+}  // namespace lp

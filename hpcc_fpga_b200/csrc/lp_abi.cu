@@ -174,7 +174,7 @@ static int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int 
 
 // Panel work of block step K: lu on the diagonal block, then the top block
 // row and the left block column (Lt written into `lt`).
-static int panel(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st) {
+int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st) {
     float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
     const double b = bs;
     int e = prof_begin(c, st);
@@ -211,7 +211,7 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
     float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + (size_t)bs * n};
     const int nb = n / bs;
     const double b = bs;
-    LP_CHECK(panel(c, dA, n, lda, bs, 0, ltbuf[0], st));
+    LP_CHECK(panel_f32(c, dA, n, lda, bs, 0, ltbuf[0], st));
     for (int K = 0; K + 1 < nb; K++) {
         const int rest = n - (K + 1) * bs;
         const double r = rest;
@@ -227,7 +227,7 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
                           inner_bytes(b, r, b) + inner_bytes(r - b, b, b)));
         LP_CUDA(cudaEventRecord(c->ev_fork, st));
         LP_CUDA(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
-        LP_CHECK(panel(c, dA, n, lda, bs, K + 1, ltbuf[(K + 1) & 1], c->aux));
+        LP_CHECK(panel_f32(c, dA, n, lda, bs, K + 1, ltbuf[(K + 1) & 1], c->aux));
         LP_CUDA(cudaEventRecord(c->ev_join, c->aux));
         if (rest > bs) {
             const double r2 = rest - bs;
@@ -309,6 +309,7 @@ int lp_ctx_create(int device, lp_ctx** out) {
     LP_CHECK(trsm_init_attrs());
     LP_CHECK(sgemm_init_attrs());
     LP_CHECK(gesl_init_attrs());
+    LP_CHECK(umma_init_attrs());
     lp_ctx* c = new lp_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
@@ -451,6 +452,71 @@ int lp_gesl_dev(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs
         return fail(LP_E_INVALID, "lp_gesl_dev: factors must be 16-byte aligned with lda a multiple of 4");
     LP_CUDA(cudaSetDevice(c->device));
     return gesl_f32(c, dLU, n, lda, dB, nrhs, ldb, c->stream);
+}
+
+int lp_gefa_prec_dev(lp_ctx* c, int precision, float* dA, int n, int lda, int bs) {
+    if (c == nullptr) return fail(LP_E_INVALID, "lp_gefa_prec_dev: null context");
+    LP_CHECK(validate_matrix(dA, n, lda, bs, "lp_gefa_prec_dev"));
+    if (!aligned16(dA)) return fail(LP_E_INVALID, "lp_gefa_prec_dev: matrix must be 16-byte aligned");
+    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR)
+        return fail(LP_E_INVALID, "lp_gefa_prec_dev: unknown precision");
+    LP_CUDA(cudaSetDevice(c->device));
+    if (precision == LP_F32) return gefa_f32(c, dA, n, lda, bs, c->stream);
+    return gefa_mixed(c, precision, dA, n, lda, bs, c->stream);
+}
+
+int lp_inner_update_tc_dev(lp_ctx* c, int precision, float* dC, int ldc, const float* dL, int ldl, const float* dT,
+                           int ldt, int m, int n, int bs) {
+    if (c == nullptr || dC == nullptr || dL == nullptr || dT == nullptr)
+        return fail(LP_E_INVALID, "lp_inner_update_tc_dev: null argument");
+    if (precision != LP_BF16_IR && precision != LP_FP8_IR)
+        return fail(LP_E_INVALID, "lp_inner_update_tc_dev: precision must be LP_BF16_IR or LP_FP8_IR");
+    const bool fp8 = precision == LP_FP8_IR;
+    if (m <= 0 || n <= 0 || m % 128 || n % 128 || bs <= 0 || bs % 128 || ldc < n || ldl < bs || ldt < n ||
+        ldl % 4 || !aligned16(dL))
+        return fail(LP_E_INVALID, "lp_inner_update_tc_dev: m, n, bs must be positive multiples of 128");
+    LP_CUDA(cudaSetDevice(c->device));
+    const size_t esz = fp8 ? 1 : 2;
+    const int nblk = ((m > n ? m : n) + 511) / 512;
+    LP_CHECK(c->q.ensure(esz * (size_t)bs * ((size_t)m + n)));
+    LP_CHECK(c->qs.ensure(6 * sizeof(float) * (size_t)nblk));
+    LP_CHECK(c->err.ensure(sizeof(int)));
+    uint8_t* aq = static_cast<uint8_t*>(c->q.ptr);
+    uint8_t* bq = aq + esz * (size_t)bs * m;
+    float* sc = static_cast<float*>(c->qs.ptr);
+    cudaStream_t st = c->stream;
+    LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
+    LP_CHECK(quantize_panel(dL, ldl, dT, ldt, m, n, bs, fp8, aq, bq, sc, nblk, st));
+    LP_CHECK(launch_umma_update(dC, ldc, aq, m, bq, n, 0, 0, m, n, bs, fp8, fp8 ? sc + nblk : nullptr,
+                                fp8 ? sc + 4 * nblk : nullptr, static_cast<int*>(c->err.ptr), st));
+    int herr = 0;
+    LP_CUDA(cudaMemcpyAsync(&herr, c->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    if (herr != 0) return fail(LP_E_TIMEOUT, "lp_inner_update_tc_dev: a bounded wait expired in the kernel");
+    return LP_OK;
+}
+
+int lp_refine_dev(lp_ctx* c, const float* dA0, int lda, const float* dLU, int n, const double* dB64, double* dX,
+                  int nrhs, int max_iters, lp_timing* t) {
+    if (c == nullptr || dA0 == nullptr || dLU == nullptr || dB64 == nullptr || dX == nullptr)
+        return fail(LP_E_INVALID, "lp_refine_dev: null argument");
+    if (n <= 0 || lda < n || lda % 4 != 0 || nrhs <= 0 || !aligned16(dLU))
+        return fail(LP_E_INVALID, "lp_refine_dev: bad sizes");
+    LP_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    LP_CUDA(cudaEventRecord(c->ev[0], st));
+    int iters = 0;
+    double resid = 0.0;
+    const int s = refine_core(c, dA0, lda, dLU, n, dB64, dX, nrhs, max_iters, &iters, &resid, st);
+    LP_CUDA(cudaEventRecord(c->ev[1], st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    if (t != nullptr) {
+        std::memset(t, 0, sizeof(*t));
+        t->ir_s = elapsed_s(c->ev[0], c->ev[1]);
+        t->ir_iters = iters;
+        t->hpl_resid = resid;
+    }
+    return s;
 }
 
 // ---- host entry points --------------------------------------------------------------

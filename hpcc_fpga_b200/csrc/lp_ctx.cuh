@@ -24,6 +24,19 @@ struct Workspace {
 
 int validate_matrix(const void* a, int n, int lda, int bs, const char* who);
 int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st);
+int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st);
+// Panel work of block step K (lu, top, left; Lt into lt), on stream st.
+int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st);
+int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
+                   uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st);
+int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
+                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
+                       cudaStream_t st);
+int umma_init_attrs();
+// x = LU \ b, then FP64 refinement against the original matrix a0 until the
+// HPL scaled residual is <= 16 or max_iters refinements were made.
+int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
+                int max_iters, int* iters, double* resid, cudaStream_t st);
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                     double* x, int max_iters, lp_timing* t);
@@ -46,6 +59,9 @@ struct lp_ctx {
     lp::Workspace lt;    // transposed left panels (2 x bs x n, alternating by block step)
     lp::Workspace dsub;  // transposed diagonal sub-blocks of the blocked top stage (per stream)
     lp::Workspace lti;   // transposed inner left panel of the recursive lu stage (per stream)
+    lp::Workspace q;     // tensor-core operands: 2 x (Lq, Tq), BF16 or E4M3, n x bs each
+    lp::Workspace qs;    // E4M3 block scales (absmax, scale, 1/scale for L and T), 2 buffers
+    lp::Workspace err;   // device error word of the tensor-core update (bounded waits)
     lp::Workspace gw;    // substitution work vectors
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
@@ -56,7 +72,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
         for (auto* w : all) w->release();
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();

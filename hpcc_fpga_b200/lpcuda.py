@@ -95,6 +95,9 @@ def lib() -> ctypes.CDLL:
     L.lp_left_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _I, _I, _VP, _I]
     L.lp_inner_update_dev.argtypes = [_VP, _VP, _I, _VP, _I, _VP, _I, _I, _I, _I]
     L.lp_gefa_dev.argtypes = [_VP, _VP, _I, _I, _I]
+    L.lp_gefa_prec_dev.argtypes = [_VP, _I, _VP, _I, _I, _I]
+    L.lp_inner_update_tc_dev.argtypes = [_VP, _I, _VP, _I, _VP, _I, _VP, _I, _I, _I, _I]
+    L.lp_refine_dev.argtypes = [_VP, _VP, _I, _VP, _I, _VP, _VP, _I, _I, ctypes.POINTER(LpTiming)]
     L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
     L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
@@ -223,6 +226,21 @@ class Context:
 
     def gefa(self, dA: int, n: int, lda: int, bs: int) -> None:
         check(lib().lp_gefa_dev(self._h, dA, n, lda, bs), "lp_gefa_dev")
+
+    def gefa_prec(self, precision: str, dA: int, n: int, lda: int, bs: int) -> None:
+        check(lib().lp_gefa_prec_dev(self._h, PRECISIONS[precision], dA, n, lda, bs), "lp_gefa_prec_dev")
+
+    def inner_update_tc(self, precision: str, dC: int, ldc: int, dL: int, ldl: int, dT: int, ldt: int, m: int,
+                        n: int, bs: int) -> None:
+        check(lib().lp_inner_update_tc_dev(self._h, PRECISIONS[precision], dC, ldc, dL, ldl, dT, ldt, m, n, bs),
+              "lp_inner_update_tc_dev")
+
+    def refine(self, dA0: int, lda: int, dLU: int, n: int, dB64: int, dX: int, nrhs: int = 1,
+               max_iters: int = 50) -> dict:
+        t = LpTiming()
+        check(lib().lp_refine_dev(self._h, dA0, lda, dLU, n, dB64, dX, nrhs, max_iters, ctypes.byref(t)),
+              "lp_refine_dev")
+        return t.as_dict()
 
     def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
         check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")

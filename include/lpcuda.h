@@ -134,12 +134,32 @@ int lp_left_update_dev(lp_ctx* ctx, const float* dLU, int ldlu, float* dL, int l
 int lp_inner_update_dev(lp_ctx* ctx, float* dC, int ldc, const float* dLt, int ldlt, const float* dT, int ldt,
                         int m, int n, int bs);
 
+/* inner on the tensor cores: C(m x n) += L(m x bs) * T(bs x n) with L and T
+ * rounded to BF16 (LP_BF16_IR) or to E4M3 with one absmax scale per 512-row
+ * block of L and 512-column block of T (LP_FP8_IR), FP32 accumulation —
+ * the mixed-precision form of inner_update_mm (hpl_torus_PCIE.cl:711-865).
+ * L is given row-major (ldl), T row-major (ldt); m, n, bs multiples of 128.
+ * Returns LP_E_TIMEOUT if a bounded wait inside the kernel expired. */
+int lp_inner_update_tc_dev(lp_ctx* ctx, int precision, float* dC, int ldc, const float* dL, int ldl,
+                           const float* dT, int ldt, int m, int n, int bs);
+
 /* ---- whole factorization and solve (device pointers) -------------------- */
 /* Blocked right-looking LU without pivoting of the n x n matrix at dA, in
  * place, in the reference encoding.  Replaces the block-row loop of
  * execution::pcie::calculate (execution_types/execution_pcie.hpp:177-641).
  * n must be a multiple of bs. */
 int lp_gefa_dev(lp_ctx* ctx, float* dA, int n, int lda, int bs);
+/* The same factorization with the trailing updates in the chosen precision
+ * (LP_F32: identical to lp_gefa_dev; LP_BF16_IR / LP_FP8_IR: tensor-core
+ * trailing updates, bs a multiple of 128; the factors stay FP32). */
+int lp_gefa_prec_dev(lp_ctx* ctx, int precision, float* dA, int n, int lda, int bs);
+/* x = LU \ b followed by FP64 iterative refinement: r = b - M x with the
+ * original FP32 matrix dA0 widened to FP64, d = LU \ r, x += d, until the
+ * HPL scaled residual (LINPACK/src/host/gmres.c:182-193, eps = DBL_EPSILON/2)
+ * is <= 16 or max_iters refinements were made.  dB64, dX: nrhs rows of n
+ * doubles.  t (optional) receives ir_s, ir_iters and hpl_resid. */
+int lp_refine_dev(lp_ctx* ctx, const float* dA0, int lda, const float* dLU, int n, const double* dB64, double* dX,
+                  int nrhs, int max_iters, lp_timing* t);
 /* Forward + back substitution with the encoded factors for nrhs right-hand
  * sides stored as rows of dB (dB[r*ldb + i]); the solutions overwrite dB.
  * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229). */

@@ -1,0 +1,124 @@
+"""Mixed-precision path: the tensor-core inner update (BF16 / FP8 E4M3 with
+512-block absmax scales, FP32 accumulation) and the full factorization with
+FP64 iterative refinement.
+
+Stage parity: C + q(L) q(T) computed in FP64 from the same rounded operands
+(rounding emulated with torch's bfloat16 / float8_e4m3fn casts, scales formed
+exactly as the kernel forms them) must match the GPU within the FP32
+accumulation bound (bs + 2) * eps32 * (|C| + |q(L)| |q(T)|).
+Solve parity: refinement must reach the HPL scaled residual <= 16
+(LINPACK/src/host/gmres.c:182-193) and the FP64-oracle error (the exact
+solution is all ones) must be small."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+FLT_EPS = float(np.finfo(np.float32).eps)
+
+
+def q_bf16(torch, x):
+    return torch.from_numpy(np.ascontiguousarray(x)).bfloat16().float().numpy().astype(np.float64)
+
+
+def q_fp8_rows(torch, L):
+    """Per 512-row block: s = amax/448, q = e4m3(L * (1/s)) dequantized."""
+    out = np.empty(L.shape, np.float64)
+    for b0 in range(0, L.shape[0], 512):
+        blk = L[b0:b0 + 512]
+        amax = np.float32(np.abs(blk).max())
+        s = np.float32(amax / np.float32(448.0)) if amax > 0 else np.float32(1.0)
+        inv = np.float32(np.float32(1.0) / s)
+        v = (blk * inv).astype(np.float32)
+        q = torch.from_numpy(np.ascontiguousarray(v)).to(torch.float8_e4m3fn).float().numpy()
+        out[b0:b0 + 512] = q.astype(np.float64) * np.float64(s)
+    return out
+
+
+@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (256, 384, 256), (640, 512, 512)])
+def test_inner_update_tc_bf16(ctx, dev, m, n, bs):
+    rng = np.random.default_rng(m + n + bs)
+    C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
+    L = rng.uniform(-1, 1, (m, bs)).astype(np.float32)
+    T = rng.uniform(-1, 1, (bs, n)).astype(np.float32)
+    dC, dL, dT = dev.put(C), dev.put(L), dev.put(T)
+    ctx.inner_update_tc("bf16", dC.data_ptr(), n, dL.data_ptr(), bs, dT.data_ptr(), n, m, n, bs)
+    got = dev.get(dC).astype(np.float64)
+    Lq, Tq = q_bf16(dev.torch, L), q_bf16(dev.torch, T)
+    exact = C.astype(np.float64) + Lq @ Tq
+    bound = (bs + 2) * FLT_EPS * (np.abs(C) + np.abs(Lq) @ np.abs(Tq))
+    assert np.all(np.abs(got - exact) <= bound)
+
+
+@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (1024, 640, 512)])
+def test_inner_update_tc_fp8(ctx, dev, m, n, bs):
+    rng = np.random.default_rng(3 * m + n + bs)
+    C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
+    L = rng.uniform(-1, 1, (m, bs)).astype(np.float32) * np.float32(3.0)
+    T = rng.uniform(-1, 1, (bs, n)).astype(np.float32) * np.float32(0.01)
+    dC, dL, dT = dev.put(C), dev.put(L), dev.put(T)
+    ctx.inner_update_tc("fp8", dC.data_ptr(), n, dL.data_ptr(), bs, dT.data_ptr(), n, m, n, bs)
+    got = dev.get(dC).astype(np.float64)
+    Lq = q_fp8_rows(dev.torch, L)
+    Tq = q_fp8_rows(dev.torch, np.ascontiguousarray(T.T)).T
+    exact = C.astype(np.float64) + Lq @ Tq
+    bound = (bs + 4) * FLT_EPS * (np.abs(C) + np.abs(Lq) @ np.abs(Tq))
+    assert np.all(np.abs(got - exact) <= bound)
+
+
+def test_gefa_prec_f32_is_gefa(ctx, dev):
+    n, bs = 1024, 256
+    A, _, _, _ = oracle.gen_reference(n)
+    d1, d2 = dev.put(A), dev.put(A)
+    ctx.gefa(d1.data_ptr(), n, n, bs)
+    ctx.gefa_prec("f32", d2.data_ptr(), n, n, bs)
+    assert np.array_equal(dev.get(d1), dev.get(d2))
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+@pytest.mark.parametrize("n,bs", [(1024, 128), (2048, 512)])
+def test_mixed_factors_close_to_fp32(ctx, dev, prec, n, bs):
+    """The rounded-update factors stay close to the FP32 ones (diagonally
+    dominant input: relative error of a few operand roundings)."""
+    A, _, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
+    d = dev.put(A)
+    ctx.gefa_prec(prec, d.data_ptr(), n, n, bs)
+    got = dev.get(d).astype(np.float64)
+    want = oracle.gefa_nopvt(A).astype(np.float64)
+    assert np.all(np.isfinite(got))
+    rel = np.abs(got - want).max() / np.abs(want).max()
+    assert rel < (2e-2 if prec == "fp8" else 2e-3)
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+@pytest.mark.parametrize("margin", ["1", "sqrt", "n"])
+def test_mixed_ir_reaches_hpl_threshold(ctx, prec, margin):
+    n, bs = 2048, 256
+    mg = {"1": 1.0, "sqrt": 0.1 * n ** 0.5, "n": float(n)}[margin]
+    A, b64, _ = oracle.gen_baseline(n, seed=42, margin=mg)
+    x, t = ctx.solve_host(A, b64, bs, prec, max_iters=50)
+    assert t["hpl_resid"] <= 16.0
+    assert oracle.hpl_resid(A, x, b64) <= 16.0
+    assert np.abs(x - 1.0).max() < 1e-9      # FP64 oracle: the exact solution is all ones
+    assert t["ir_iters"] >= 1
+
+
+def test_refine_dev_on_resident_factors(ctx, dev):
+    n, bs = 1024, 128
+    A, b64, _ = oracle.gen_baseline(n, seed=5, margin=1.0)
+    dA0, dLU = dev.put(A), dev.put(A)
+    ctx.gefa_prec("bf16", dLU.data_ptr(), n, n, bs)
+    dB = dev.put(np.stack([b64, 2.0 * b64]))
+    dX = dev.empty((2, n), np.float64)
+    t = ctx.refine(dA0.data_ptr(), n, dLU.data_ptr(), n, dB.data_ptr(), dX.data_ptr(), nrhs=2, max_iters=50)
+    X = dev.get(dX)
+    assert t["hpl_resid"] <= 16.0
+    assert np.abs(X[0] - 1.0).max() < 1e-9 and np.abs(X[1] - 2.0).max() < 2e-9
+
+
+def test_mixed_rejects_small_block(ctx, lp):
+    A = np.eye(256, dtype=np.float32) * 2
+    with pytest.raises(lp.LpError) as e:
+        ctx.solve_host(A, np.ones(256), 64, "bf16")
+    assert e.value.status == lp.LP_E_INVALID
