@@ -123,6 +123,61 @@ def cpu_baseline(n: int, reps: int) -> dict:
             "t_min_s": r["t_min"], "host_nproc": os.cpu_count()}
 
 
+def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, f32_value, pk) -> dict:
+    """BF16 / FP8 trailing updates + FP64 refinement to the HPL threshold on
+    the same system: GFLOP/s by the same formula over factor + all solves +
+    refinement (the refinement's own 2n^2 flop per iteration not credited)."""
+    with torch.cuda.stream(stream):
+        dB64 = torch.from_numpy(b64).to("cuda")
+        dX = torch.empty(n, dtype=torch.float64, device="cuda")
+    info = {}
+
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+        ctx.gefa_prec(prec, dA.data_ptr(), n, n, bs)
+        info.update(ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dX.data_ptr(), 1, 50))
+
+    for _ in range(warmup):
+        step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.read_profile(reset=True)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    iters = []
+    resid = []
+    for _ in range(steps):
+        step()
+        iters.append(info["ir_iters"])
+        resid.append(info["hpl_resid"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    prof = ctx.read_profile(reset=True)
+    ctx.set_profiling(False)
+    x = dX.cpu().numpy()
+    inner = prof["inner"]
+    gbs = inner["bytes"] / inner["s"] / 1e9 if inner["s"] > 0 else None
+    tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
+    value = steps * flops(n) / t / 1e9
+    return {
+        "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32": value / f32_value,
+        "ir_iters": max(iters), "hpl_resid": max(resid), "hpl_eps": "DBL_EPSILON/2",
+        "max_abs_err_vs_fp64_oracle": float(np.abs(x - 1.0).max()),
+        "roofline": {"bound": "hbm", "kernel": f"k_umma_update<{prec}> (inner stage, tcgen05)",
+                     "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": gbs / pk["hbm_gbs"] if gbs else None,
+                     "per_unit": "8*m*n bytes (FP32 C read+write) per m x n trailing update; "
+                                 "2*m*n*bs flop, intensity bs/4 flop/B below the BF16 ridge",
+                     "tensor_tflops": tfs, "tensor_peak_tflops": pk["bf16_tflops"],
+                     "peak_source": pk["source"]},
+        "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]},
+    }
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -167,6 +222,7 @@ def main() -> None:
     ap.add_argument("--cpu-reps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -230,6 +286,13 @@ def main() -> None:
     ctx.set_profiling(False)
     x = dB.cpu().numpy()
     max_err = float(np.abs(x.astype(np.float64) - 1.0).max())
+    # HPL scaled residual of the plain FP32 solution (no refinement), in both
+    # unit roundoffs, for the equal-residual comparison with the mixed forms.
+    with torch.cuda.stream(stream):
+        dB64r = torch.from_numpy(b64).to("cuda")
+        dXr = torch.empty(n, dtype=torch.float64, device="cuda")
+    r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64r.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
+    del dB64r, dXr
     t_max = elapsed
     if world > 1:
         t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
@@ -245,6 +308,12 @@ def main() -> None:
     stage_share = {k: prof[k]["s"] / max(1e-12, sum(prof[s]["s"] for s in lp.STAGES)) for k in lp.STAGES}
     gesl = prof["gesl"]
     pk = peaks()
+
+    mixed = {}
+    if not args.no_mixed and bs % 128 == 0:
+        for prec in ("bf16", "fp8"):
+            mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, args.steps,
+                                    max(1, min(args.warmup, 2)), value / world, pk)
 
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
@@ -292,6 +361,9 @@ def main() -> None:
                    "l2": f"inputs larger than L2 ({4 * n * n / 2**30:.1f} GiB matrix, restored every step)",
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
         "max_abs_err_x": max_err,
+        "hpl_resid": {"eps_dbl_half": r32, "eps_flt_half": r32 * 2.0 ** -29,
+                      "note": "plain FP32 solution, HPL scaled residual (gmres.c:182-193) with eps = 2^-53 and "
+                              "with the FP32 unit roundoff 2^-24"},
         "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)",
                      "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
                      "frac": (achieved_tf / peak_tf) if achieved_tf else None,
@@ -307,6 +379,8 @@ def main() -> None:
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if mixed:
+        line["mixed"] = mixed
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu:

@@ -243,8 +243,11 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
 
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st) {
     LP_CHECK(c->gw.ensure(sizeof(float) * gesl_work_floats(n, nrhs)));
+    LP_CHECK(c->ginv.ensure(sizeof(float) * gesl_inv_floats(n)));
+    float* inv = static_cast<float*>(c->ginv.ptr);
     const int e = prof_begin(c, st);
-    LP_CHECK(launch_gesl(dLU, lda, n, dB, ldb, nrhs, static_cast<float*>(c->gw.ptr), st));
+    LP_CHECK(launch_diag_inverses(dLU, lda, n, inv, st));
+    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, static_cast<float*>(c->gw.ptr), inv, st));
     const double nn = n;
     return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
 }
@@ -309,6 +312,7 @@ int lp_ctx_create(int device, lp_ctx** out) {
     LP_CHECK(trsm_init_attrs());
     LP_CHECK(sgemm_init_attrs());
     LP_CHECK(gesl_init_attrs());
+    LP_CHECK(gesl_inv_init_attrs());
     LP_CHECK(umma_init_attrs());
     lp_ctx* c = new lp_ctx();
     c->device = device;

@@ -47,6 +47,12 @@ int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, i
 // Forward + back substitution for nrhs rows of b (see k_gesl.cu).
 int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t s);
 size_t gesl_work_floats(int n, int nrhs);
+// The same with precomputed inverses of the 128 x 128 diagonal blocks (k_gesl_inv.cu).
+int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_t s);
+int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
+                    cudaStream_t s);
+size_t gesl_inv_floats(int n);
+int gesl_inv_init_attrs();
 // FP64 refinement pieces (see k_ir.cu).
 int launch_residual_f64(const float* a, int lda, int n, const double* x, int ldx, const double* b, int ldb,
                         double* r, int ldr, int nrhs, cudaStream_t s);

@@ -63,6 +63,7 @@ struct lp_ctx {
     lp::Workspace qs;    // E4M3 block scales (absmax, scale, 1/scale for L and T), 2 buffers
     lp::Workspace err;   // device error word of the tensor-core update (bounded waits)
     lp::Workspace gw;    // substitution work vectors
+    lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
     bool prof_on = false;
@@ -72,7 +73,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
         for (auto* w : all) w->release();
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();

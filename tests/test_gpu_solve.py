@@ -59,9 +59,9 @@ def test_baseline_inputs_hpl_residual(ctx, n, bs):
     assert np.abs(x - 1.0).max() <= 4 * np.abs(x_cpu - 1.0).max() + 1e-6
 
 
-@pytest.mark.parametrize("nrhs", [1, 3, 16, 17])
-def test_gesl_multi_rhs(ctx, dev, nrhs):
-    n, bs = 384, 128
+@pytest.mark.parametrize("n,nrhs", [(384, 1), (384, 3), (384, 16), (384, 17), (300, 2), (4, 1), (1000, 5)])
+def test_gesl_multi_rhs(ctx, dev, n, nrhs):
+    """Ragged n (not a multiple of the 128-wide substitution blocks) included."""
     A, _, _, _ = oracle.gen_reference(n)
     LU = oracle.gefa_nopvt(A)
     rng = np.random.default_rng(nrhs)
