@@ -1,0 +1,395 @@
+// Batched factor + solve of many independent systems in ONE persistent launch.
+//
+// Each system i is an n_i x n_i matrix in the reference encoding
+// (LINPACK/src/host/linpack_data.cpp:166-229: factored in place, diagonal
+// -1/u_kk, negated multipliers in storage rows, U in storage columns) with
+// nrhs_i right-hand sides stored as rows of B_i, overwritten by the
+// solutions.  CTAs pull systems from an atomic counter over a list sorted by
+// decreasing n (largest first: the slowest systems start first, the small
+// ones fill the tail), so one launch balances any size mix.
+//
+// Per system, one CTA of 256 threads:
+//   n <= small_n_max (<= 128): the whole matrix and right-hand sides in
+//     shared memory; right-looking LU with one barrier per step, then the
+//     forward and back sweeps.
+//   larger n: blocked right-looking LU with panel width NB (16 or 32, per
+//     size bucket, chosen by the autotuner): the diagonal block factored in
+//     shared memory; the top block row (column-independent) and left block
+//     column (row-independent) by their recurrences in registers; the
+//     trailing update as 64 x 64 register-tiled tiles through shared memory.
+//     (Panel widths 16 and 32 keep a column's recurrence in registers.)
+//     Then blocked forward/back sweeps with the right-hand sides resident in
+//     shared memory and each diagonal block staged before its sequential solve.
+// Arithmetic uses fused multiply-add: results agree with the reference to
+// rounding (checked against the oracle in tests/test_gpu_batch.py).
+#include "lp_ctx.cuh"
+
+namespace lp {
+namespace {
+
+constexpr int BT = 256;
+constexpr int SMALL_MAX = 128;
+constexpr int RHS_MAX = 16;
+constexpr int TILE = 64;
+constexpr int NBUCKETS = 5;
+
+struct BatchSys {
+    int n, nrhs, lda, ldb;
+    long long a_off, b_off;
+};
+static_assert(sizeof(BatchSys) == sizeof(lp_system), "lp_system layout");
+
+struct Tune {
+    int small_n_max;
+    int nb[NBUCKETS];
+};
+
+constexpr size_t kSmallFloats = (size_t)SMALL_MAX * (SMALL_MAX + 1) + (size_t)RHS_MAX * SMALL_MAX;
+constexpr size_t kBlockedFloats = (size_t)RHS_MAX * 1024;  // right-hand sides of n <= 1024 in the solve phase
+constexpr size_t kBatchSmem = sizeof(float) * (kSmallFloats > kBlockedFloats ? kSmallFloats : kBlockedFloats);
+
+__device__ __forceinline__ int bucket_of(int n) {
+    return n <= 64 ? 0 : n <= 128 ? 1 : n <= 256 ? 2 : n <= 512 ? 3 : 4;
+}
+
+// In-place LU (reference encoding) of an m x m matrix in shared memory with
+// row stride ld, all threads of the CTA; one barrier per step.
+__device__ void smem_lu(float* S, int ld, int m) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float inv_prev = 0.0f;
+    for (int k = 0; k < m; k++) {
+        const float inv = (float)(-1.0 / (double)S[k * ld + k]);
+        if (k > 0) {
+            float* rp = S + (k - 1) * ld;
+            for (int i = k + tid; i < m; i += BT) rp[i] *= inv_prev;
+            if (tid == 0) rp[k - 1] = inv_prev;
+        }
+        const float* rk = S + k * ld;
+        for (int i0 = k + 1; i0 < m; i0 += 32) {
+            const int i = i0 + lane;
+            const float sc = (i < m) ? rk[i] * inv : 0.0f;
+            for (int j = k + 1 + warp; j < m; j += BT / 32) {
+                float* rj = S + j * ld;
+                if (i < m) rj[i] = fmaf(sc, rj[k], rj[i]);
+            }
+        }
+        inv_prev = inv;
+        __syncthreads();
+    }
+    if (tid == 0 && m > 0) S[(m - 1) * ld + (m - 1)] = inv_prev;
+    __syncthreads();
+}
+
+// Forward/back sweeps on right-hand sides Y (nrhs rows of length m, stride m)
+// with the factors in shared memory (row stride ld).
+__device__ void smem_solve(const float* S, int ld, int m, float* Y, int nrhs, float* sc) {
+    const int tid = threadIdx.x;
+    for (int k = 0; k + 1 < m; k++) {
+        for (int idx = tid; idx < nrhs * m; idx += BT) {
+            const int q = idx / m, i = idx - q * m;
+            if (i > k) Y[idx] = fmaf(Y[q * m + k], S[k * ld + i], Y[idx]);
+        }
+        __syncthreads();
+    }
+    for (int k = m - 1; k >= 0; k--) {
+        if (tid < nrhs) sc[tid] = Y[tid * m + k] * S[k * ld + k];
+        __syncthreads();
+        for (int idx = tid; idx < nrhs * m; idx += BT) {
+            const int q = idx / m, i = idx - q * m;
+            if (i < k)
+                Y[idx] = fmaf(sc[q], S[k * ld + i], Y[idx]);
+            else if (i == k)
+                Y[idx] = -sc[q];
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
+    const int ld = n | 1;  // odd stride: column reads hit distinct banks
+    float* S = sm;
+    float* Y = sm + SMALL_MAX * (SMALL_MAX + 1);
+    __shared__ float sc[RHS_MAX];
+    for (int idx = threadIdx.x; idx < n * n; idx += BT) {
+        const int r = idx / n, c = idx - r * n;
+        S[r * ld + c] = a[(size_t)r * lda + c];
+    }
+    for (int idx = threadIdx.x; idx < nrhs * n; idx += BT) {
+        const int q = idx / n, i = idx - q * n;
+        Y[idx] = b[(size_t)q * ldb + i];
+    }
+    __syncthreads();
+    smem_lu(S, ld, n);
+    smem_solve(S, ld, n, Y, nrhs, sc);
+    for (int idx = threadIdx.x; idx < n * n; idx += BT) {
+        const int r = idx / n, c = idx - r * n;
+        a[(size_t)r * lda + c] = S[r * ld + c];
+    }
+    for (int idx = threadIdx.x; idx < nrhs * n; idx += BT) {
+        const int q = idx / n, i = idx - q * n;
+        b[(size_t)q * ldb + i] = Y[idx];
+    }
+    __syncthreads();
+}
+
+// Blocked factorization of one system in global memory (see file comment).
+template <int NB>
+__device__ void factor_blocked(float* a, int lda, int n, float* sm) {
+    constexpr int DL = NB + 1;
+    float* Ds = sm;                         // NB x (NB+1) diagonal block
+    float* Lt = Ds + NB * DL;               // NB x (TILE+1): left tile, k-major
+    float* Ts = Lt + NB * (TILE + 1);       // NB x TILE: top tile
+    const int tid = threadIdx.x;
+    for (int k0 = 0; k0 < n; k0 += NB) {
+        const int kb = min(NB, n - k0);
+        const int r0 = k0 + kb, rem = n - r0;
+        float* d = a + (size_t)k0 * lda + k0;
+        for (int idx = tid; idx < kb * kb; idx += BT) {
+            const int r = idx / kb, c = idx - r * kb;
+            Ds[r * DL + c] = d[(size_t)r * lda + c];
+        }
+        __syncthreads();
+        smem_lu(Ds, DL, kb);
+        for (int idx = tid; idx < kb * kb; idx += BT) {
+            const int r = idx / kb, c = idx - r * kb;
+            d[(size_t)r * lda + c] = Ds[r * DL + c];
+        }
+        if (rem <= 0) {
+            __syncthreads();
+            break;
+        }
+        // top: every column c of the block row, t_k *= D_kk; t_j += t_k D_jk (j > k)
+        for (int c = r0 + tid; c < n; c += BT) {
+            float x[NB];
+#pragma unroll
+            for (int i = 0; i < NB; i++) x[i] = (i < kb) ? a[(size_t)(k0 + i) * lda + c] : 0.0f;
+#pragma unroll
+            for (int k = 0; k < NB; k++) {
+                if (k < kb) {
+                    const float xk = x[k] * Ds[k * DL + k];
+                    x[k] = xk;
+#pragma unroll
+                    for (int j = k + 1; j < NB; j++) x[j] = fmaf(xk, Ds[j * DL + k], x[j]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < NB; i++)
+                if (i < kb) a[(size_t)(k0 + i) * lda + c] = x[i];
+        }
+        // left: every row rr of the block column, l_i += l_k D_ki (i > k)
+        for (int rr = r0 + tid; rr < n; rr += BT) {
+            float x[NB];
+            float* row = a + (size_t)rr * lda + k0;
+#pragma unroll
+            for (int i = 0; i < NB; i++) x[i] = (i < kb) ? row[i] : 0.0f;
+#pragma unroll
+            for (int k = 0; k < NB; k++)
+#pragma unroll
+                for (int i = k + 1; i < NB; i++) x[i] = fmaf(x[k], Ds[k * DL + i], x[i]);
+#pragma unroll
+            for (int i = 0; i < NB; i++)
+                if (i < kb) row[i] = x[i];
+        }
+        __syncthreads();
+        // inner: C[r0:n, r0:n] += L * T, 64 x 64 tiles, 4 x 4 per thread
+        const int ty = tid >> 4, tx = tid & 15;
+        const int tiles = (rem + TILE - 1) / TILE;
+        for (int t = 0; t < tiles * tiles; t++) {
+            const int ti = t / tiles, tj = t - ti * tiles;
+            const int m0 = r0 + ti * TILE, c0 = r0 + tj * TILE;
+            for (int idx = tid; idx < TILE * kb; idx += BT) {
+                const int i = idx / kb, k = idx - i * kb;
+                Lt[k * (TILE + 1) + i] = (m0 + i < n) ? a[(size_t)(m0 + i) * lda + k0 + k] : 0.0f;
+            }
+            for (int idx = tid; idx < kb * TILE; idx += BT) {
+                const int k = idx / TILE, j = idx - k * TILE;
+                Ts[k * TILE + j] = (c0 + j < n) ? a[(size_t)(k0 + k) * lda + c0 + j] : 0.0f;
+            }
+            __syncthreads();
+            float acc[4][4];
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[p][q] = 0.0f;
+            for (int k = 0; k < kb; k++) {
+                const float* lrow = Lt + k * (TILE + 1) + ty * 4;
+                const float4 tv = *reinterpret_cast<const float4*>(Ts + k * TILE + tx * 4);
+                const float lv[4] = {lrow[0], lrow[1], lrow[2], lrow[3]};
+                const float tvv[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+                for (int p = 0; p < 4; p++)
+#pragma unroll
+                    for (int q = 0; q < 4; q++) acc[p][q] = fmaf(lv[p], tvv[q], acc[p][q]);
+            }
+#pragma unroll
+            for (int p = 0; p < 4; p++) {
+                const int r = m0 + ty * 4 + p;
+                if (r >= n) continue;
+                float* crow = a + (size_t)r * lda + c0 + tx * 4;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (c0 + tx * 4 + q < n) crow[q] += acc[p][q];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// Blocked forward/back sweeps, right-hand sides resident in shared memory.
+__device__ void solve_blocked(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
+    constexpr int SBK = 64, DL = SBK + 1;
+    float* Y = sm;                       // nrhs x n
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    __shared__ float Dblk[SBK * DL];
+    __shared__ float scq[RHS_MAX];
+    for (int idx = tid; idx < nrhs * n; idx += BT) {
+        const int q = idx / n, i = idx - q * n;
+        Y[idx] = b[(size_t)q * ldb + i];
+    }
+    __syncthreads();
+    // forward: y_i += y_k S[k][i] (i > k)
+    for (int k0 = 0; k0 < n; k0 += SBK) {
+        const int kb = min(SBK, n - k0);
+        for (int idx = tid; idx < kb * kb; idx += BT) {
+            const int r = idx / kb, c = idx - r * kb;
+            Dblk[r * DL + c] = a[(size_t)(k0 + r) * lda + k0 + c];
+        }
+        __syncthreads();
+        for (int q = warp; q < nrhs; q += BT / 32) {
+            float* y = Y + q * n + k0;
+            float v0 = lane < kb ? y[lane] : 0.0f, v1 = lane + 32 < kb ? y[lane + 32] : 0.0f;
+            for (int k = 0; k < kb; k++) {
+                const float yk = __shfl_sync(0xffffffffu, k < 32 ? v0 : v1, k & 31);
+                if (lane > k && lane < kb) v0 = fmaf(yk, Dblk[k * DL + lane], v0);
+                if (lane + 32 > k && lane + 32 < kb) v1 = fmaf(yk, Dblk[k * DL + lane + 32], v1);
+            }
+            if (lane < kb) y[lane] = v0;
+            if (lane + 32 < kb) y[lane + 32] = v1;
+        }
+        __syncthreads();
+        for (int i = k0 + kb + tid; i < n; i += BT) {
+            float acc[RHS_MAX];
+#pragma unroll
+            for (int q = 0; q < RHS_MAX; q++) acc[q] = 0.0f;
+            for (int k = 0; k < kb; k++) {
+                const float s = a[(size_t)(k0 + k) * lda + i];
+#pragma unroll
+                for (int q = 0; q < RHS_MAX; q++)
+                    if (q < nrhs) acc[q] = fmaf(Y[q * n + k0 + k], s, acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < RHS_MAX; q++)
+                if (q < nrhs) Y[q * n + i] += acc[q];
+        }
+        __syncthreads();
+    }
+    // backward: s = y_k S[k][k]; x_k = -s; y_i += s S[k][i] (i < k)
+    for (int k0 = ((n - 1) / SBK) * SBK; k0 >= 0; k0 -= SBK) {
+        const int kb = min(SBK, n - k0);
+        for (int idx = tid; idx < kb * kb; idx += BT) {
+            const int r = idx / kb, c = idx - r * kb;
+            Dblk[r * DL + c] = a[(size_t)(k0 + r) * lda + k0 + c];
+        }
+        __syncthreads();
+        for (int q = warp; q < nrhs; q += BT / 32) {
+            float* y = Y + q * n + k0;
+            float v0 = lane < kb ? y[lane] : 0.0f, v1 = lane + 32 < kb ? y[lane + 32] : 0.0f;
+            for (int k = kb - 1; k >= 0; k--) {
+                const float yk = __shfl_sync(0xffffffffu, k < 32 ? v0 : v1, k & 31);
+                const float s = yk * Dblk[k * DL + k];
+                if (lane == (k & 31)) {
+                    if (k < 32) v0 = -s; else v1 = -s;
+                }
+                if (lane < k) v0 = fmaf(s, Dblk[k * DL + lane], v0);
+                if (lane + 32 < k) v1 = fmaf(s, Dblk[k * DL + lane + 32], v1);
+            }
+            if (lane < kb) y[lane] = v0;
+            if (lane + 32 < kb) y[lane + 32] = v1;
+        }
+        __syncthreads();
+        // coefficients s_k = -x_k of this block update the unknowns before it
+        for (int i = tid; i < k0; i += BT) {
+            float acc[RHS_MAX];
+#pragma unroll
+            for (int q = 0; q < RHS_MAX; q++) acc[q] = 0.0f;
+            for (int k = 0; k < kb; k++) {
+                const float s = a[(size_t)(k0 + k) * lda + i];
+#pragma unroll
+                for (int q = 0; q < RHS_MAX; q++)
+                    if (q < nrhs) acc[q] = fmaf(-Y[q * n + k0 + k], s, acc[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < RHS_MAX; q++)
+                if (q < nrhs) Y[q * n + i] += acc[q];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < nrhs * n; idx += BT) {
+        const int q = idx / n, i = idx - q * n;
+        b[(size_t)q * ldb + i] = Y[idx];
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(BT, 2) k_batch_solve(const BatchSys* __restrict__ sys, int count, float* A, float* B,
+                                                    int* next, Tune tune) {
+    extern __shared__ float sm[];
+    __shared__ int s_item;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(next, 1);
+        __syncthreads();
+        const int t = s_item;
+        __syncthreads();
+        if (t >= count) break;
+        const BatchSys s = sys[t];
+        float* a = A + s.a_off;
+        float* b = B + s.b_off;
+        if (s.n <= tune.small_n_max) {
+            solve_small(a, s.lda, s.n, b, s.ldb, s.nrhs, sm);
+        } else {
+            if (tune.nb[bucket_of(s.n)] == 16)
+                factor_blocked<16>(a, s.lda, s.n, sm);
+            else
+                factor_blocked<32>(a, s.lda, s.n, sm);
+            solve_blocked(a, s.lda, s.n, b, s.ldb, s.nrhs, sm);
+        }
+    }
+}
+
+}  // namespace
+
+int batch_init_attrs() {
+    LP_CUDA(cudaFuncSetAttribute(k_batch_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBatchSmem));
+    return LP_OK;
+}
+
+int validate_batch(int count, const lp_system* systems) {
+    if (count < 0 || (count > 0 && systems == nullptr)) return fail(LP_E_INVALID, "batch: bad system list");
+    for (int i = 0; i < count; i++) {
+        const lp_system& s = systems[i];
+        if (s.n <= 0 || s.n > 1024 || s.nrhs <= 0 || s.nrhs > RHS_MAX || s.lda < s.n || s.ldb < s.n || s.a_off < 0 ||
+            s.b_off < 0)
+            return fail(LP_E_INVALID, "batch: system " + std::to_string(i) +
+                                          " needs 1 <= n <= 1024, 1 <= nrhs <= 16, lda >= n, ldb >= n");
+    }
+    return LP_OK;
+}
+
+int launch_batch(lp_ctx* c, const lp_system* d_sorted, int count, float* dA, float* dB, const lp_batch_config& cfg,
+                 int* d_next, cudaStream_t st) {
+    Tune tune;
+    tune.small_n_max = cfg.small_n_max;
+    for (int i = 0; i < NBUCKETS; i++) tune.nb[i] = cfg.nb[i];
+    const int per_sm = cfg.ctas_per_sm < 1 ? 1 : (cfg.ctas_per_sm > 3 ? 3 : cfg.ctas_per_sm);
+    int grid = c->num_sms * per_sm;
+    if (grid > count) grid = count;
+    if (grid < 1) return LP_OK;
+    LP_CUDA(cudaMemsetAsync(d_next, 0, sizeof(int), st));
+    k_batch_solve<<<grid, BT, kBatchSmem, st>>>(reinterpret_cast<const BatchSys*>(d_sorted), count, dA, dB, d_next,
+                                                 tune);
+    count_launch();
+    LP_CUDA(cudaGetLastError());
+    return LP_OK;
+}
+
+}  // namespace lp

@@ -33,6 +33,7 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
                        int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
                        cudaStream_t st);
 int umma_init_attrs();
+int batch_init_attrs();
 // x = LU \ b, then FP64 refinement against the original matrix a0 until the
 // HPL scaled residual is <= 16 or max_iters refinements were made.
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
@@ -66,6 +67,12 @@ struct lp_ctx {
     lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
+    lp::Workspace bsys, bnext;                // batched: sorted system descriptors, work counter
+    lp::Workspace tA, tB;                     // batched autotuner: scratch copies of the inputs
+    uint64_t bsys_hash = 0;                   // descriptors + configuration of the cached graph
+    cudaGraphExec_t bgraph = nullptr;         // batched launch, captured once, replayed
+    lp_batch_config bcfg{};                   // autotuned configuration
+    bool btuned = false;
     bool prof_on = false;
     std::vector<cudaEvent_t> prof_ev;         // event pool, reused after every read
     size_t prof_used = 0;
@@ -73,8 +80,11 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol};
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
+                                &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
+        if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
+        bgraph = nullptr;
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();
     }

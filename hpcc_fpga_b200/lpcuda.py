@@ -58,6 +58,26 @@ class LpProfile(ctypes.Structure):
         return d
 
 
+class LpSystem(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("nrhs", ctypes.c_int), ("lda", ctypes.c_int), ("ldb", ctypes.c_int),
+                ("a_off", ctypes.c_longlong), ("b_off", ctypes.c_longlong)]
+
+
+class LpBatchConfig(ctypes.Structure):
+    _fields_ = [("small_n_max", ctypes.c_int), ("nb", ctypes.c_int * 5), ("ctas_per_sm", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"small_n_max": self.small_n_max, "nb": list(self.nb), "ctas_per_sm": self.ctas_per_sm}
+
+
+class LpBatchStats(ctypes.Structure):
+    _fields_ = [("seconds", ctypes.c_double), ("flops", ctypes.c_double), ("gflops", ctypes.c_double),
+                ("solves_per_s", ctypes.c_double), ("systems", ctypes.c_int), ("graph_replayed", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
 class LpError(RuntimeError):
     def __init__(self, status: int, where: str, detail: str):
         self.status = status
@@ -102,6 +122,10 @@ def lib() -> ctypes.CDLL:
     L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
     L.lp_solve_host.argtypes = [_VP, _I, _I, _I, _F32P, _I, _F64P, _I, _F64P, _I, ctypes.POINTER(LpTiming)]
+    L.lp_batch_default_config.argtypes = [ctypes.POINTER(LpBatchConfig)]
+    L.lp_batch_solve_dev.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig),
+                                     ctypes.POINTER(LpBatchStats)]
+    L.lp_batch_autotune.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig)]
     L.lp_generate_reference.argtypes = [_F32P, _F32P, _I, _I, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float)]
     L.lp_generate_baseline.argtypes = [_F32P, _VP, _VP, _I, ctypes.c_uint, ctypes.c_double]
@@ -244,6 +268,21 @@ class Context:
 
     def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
         check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")
+
+    # ---- batched solves ---------------------------------------------------
+    def batch_solve(self, systems, dA: int, dB: int, cfg: "LpBatchConfig | None" = None) -> dict:
+        arr = (LpSystem * len(systems))(*systems)
+        st = LpBatchStats()
+        check(lib().lp_batch_solve_dev(self._h, len(systems), arr, dA, dB,
+                                       ctypes.byref(cfg) if cfg is not None else None, ctypes.byref(st)),
+              "lp_batch_solve_dev")
+        return st.as_dict()
+
+    def batch_autotune(self, systems, dA: int, dB: int) -> LpBatchConfig:
+        arr = (LpSystem * len(systems))(*systems)
+        cfg = LpBatchConfig()
+        check(lib().lp_batch_autotune(self._h, len(systems), arr, dA, dB, ctypes.byref(cfg)), "lp_batch_autotune")
+        return cfg
 
     # ---- host entry points ------------------------------------------------
     def calculate(self, A: np.ndarray, b: np.ndarray, bs: int, repetitions: int = 1):

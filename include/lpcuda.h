@@ -205,6 +205,44 @@ int lp_calculate(lp_ctx* ctx, int n, int lda, int bs, int repetitions, float* A,
 int lp_solve_host(lp_ctx* ctx, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                   double* x, int max_iters, lp_timing* t);
 
+/* ---- batched solves (addition: no counterpart in the reference) ------------
+ * Many independent diagonally dominant systems (1 <= n <= 1024, 1 <= nrhs
+ * <= 16) factored in place (reference encoding) and solved in ONE persistent
+ * launch, captured in a CUDA graph and replayed when the same batch comes
+ * again.  System i: A_i at dA + a_off (n x n, leading dimension lda), right-
+ * hand sides at dB + b_off (nrhs rows of ldb floats), overwritten by X_i. */
+typedef struct {
+    int n, nrhs, lda, ldb;
+    long long a_off, b_off;
+} lp_system;
+/* Tuning of the batched kernel: systems with n <= small_n_max (<= 128) are
+ * solved whole in shared memory; larger ones with panel width nb[bucket]
+ * (16 or 32) for the buckets n <= 64, 128, 256, 512, 1024; ctas_per_sm
+ * persistent CTAs per SM (1..3). */
+typedef struct {
+    int small_n_max;
+    int nb[5];
+    int ctas_per_sm;
+} lp_batch_config;
+typedef struct {
+    double seconds;      /* device time of the launch (CUDA events) */
+    double flops;        /* sum over systems of 2n^3/3 + 2*nrhs*n^2 */
+    double gflops;
+    double solves_per_s; /* systems per second */
+    int systems;
+    int graph_replayed;  /* 1 if an instantiated CUDA graph was replayed */
+} lp_batch_stats;
+int lp_batch_default_config(lp_batch_config* cfg);
+/* cfg NULL: the configuration found by the last lp_batch_autotune on this
+ * context, else the default. */
+int lp_batch_solve_dev(lp_ctx* ctx, int count, const lp_system* systems, float* dA, float* dB,
+                       const lp_batch_config* cfg, lp_batch_stats* stats);
+/* Times candidate configurations per size bucket on copies of the batch
+ * (dA, dB are not modified) and returns the fastest in out; the result also
+ * becomes the context's default for lp_batch_solve_dev(cfg = NULL). */
+int lp_batch_autotune(lp_ctx* ctx, int count, const lp_system* systems, const float* dA, const float* dB,
+                      lp_batch_config* out);
+
 /* ---- input generation (host only, no GPU needed) ------------------------ */
 /* LinpackBenchmark::generateInputData for one rank
  * (LINPACK/src/host/linpack_benchmark.hpp:211-297): mt19937(0),
