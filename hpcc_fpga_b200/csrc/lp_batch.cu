@@ -98,6 +98,7 @@ int lp_batch_default_config(lp_batch_config* cfg) {
     cfg->small_n_max = 128;
     for (int i = 0; i < 5; i++) cfg->nb[i] = 32;
     cfg->ctas_per_sm = 2;
+    cfg->use_graph = 1;
     return LP_OK;
 }
 
@@ -120,7 +121,7 @@ int lp_batch_solve_dev(lp_ctx* c, int count, const lp_system* systems, float* dA
     cudaStream_t st = c->stream;
     LP_CUDA(cudaEventRecord(c->ev[0], st));
     int replayed = 0;
-    LP_CHECK(run_batch(c, sorted, dA, dB, use, true, &replayed));
+    LP_CHECK(run_batch(c, sorted, dA, dB, use, use.use_graph != 0, &replayed));
     LP_CUDA(cudaEventRecord(c->ev[1], st));
     LP_CUDA(cudaStreamSynchronize(st));
     if (stats != nullptr) {

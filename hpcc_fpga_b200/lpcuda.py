@@ -64,10 +64,12 @@ class LpSystem(ctypes.Structure):
 
 
 class LpBatchConfig(ctypes.Structure):
-    _fields_ = [("small_n_max", ctypes.c_int), ("nb", ctypes.c_int * 5), ("ctas_per_sm", ctypes.c_int)]
+    _fields_ = [("small_n_max", ctypes.c_int), ("nb", ctypes.c_int * 5), ("ctas_per_sm", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
 
     def as_dict(self) -> dict:
-        return {"small_n_max": self.small_n_max, "nb": list(self.nb), "ctas_per_sm": self.ctas_per_sm}
+        return {"small_n_max": self.small_n_max, "nb": list(self.nb), "ctas_per_sm": self.ctas_per_sm,
+                "use_graph": self.use_graph}
 
 
 class LpBatchStats(ctypes.Structure):

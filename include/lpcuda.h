@@ -223,6 +223,7 @@ typedef struct {
     int small_n_max;
     int nb[5];
     int ctas_per_sm;
+    int use_graph;       /* 1: capture the launch in a CUDA graph and replay it for the same batch */
 } lp_batch_config;
 typedef struct {
     double seconds;      /* device time of the launch (CUDA events) */
