@@ -249,6 +249,39 @@ def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
 FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
 
 
+def run_serving(lp, rates, precisions, master_n=8192) -> dict:
+    """The serving workload: Poisson arrivals at each rate of the ladder, n
+    log-uniform in [64, 8192], 1..16 right-hand sides, 30% of the requests
+    naming a matrix submitted before, 80 GB budget; continuous batching
+    against the per-request baseline (one request at a time, plain
+    launches), per precision.  Latency = completion - submission, measured
+    by the server's steady clock; solves/s over the first submission to the
+    last completion of each replay."""
+    from hpcc_fpga_b200 import serve
+
+    def count_for_rate(r):
+        return int(min(2000, max(300, 1.5 * r)))
+
+    wl = serve.Workload(master_n=master_n, seed=42)
+    out = {"workload": f"Poisson arrivals, n log-uniform in [64,{master_n}], 1-16 RHS, 30% reuse of one of the "
+                       f"last 64 matrices, principal submatrices of a seed-42 diagonally dominant {master_n}^2 "
+                       "matrix, 80 GB budget",
+           "rates": list(rates)}
+    try:
+        for prec in precisions:
+            res = {}
+            for mode in ("per_request", "continuous"):
+                t0 = time.perf_counter()
+                res[mode] = serve.ladder(lambda: lp.Server(0, precision=prec, mode=mode), wl, rates,
+                                         count_for_rate, seed=7)
+                res[mode + "_wall_s"] = round(time.perf_counter() - t0, 1)
+            res["equal_p99"] = serve.equal_p99(res["per_request"], res["continuous"])
+            out[prec] = res
+    finally:
+        wl.close()
+    return out
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
@@ -296,6 +329,9 @@ def main() -> None:
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-rates", default="100,300,1000,3000,10000,20000")
+    ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,6 +428,10 @@ def main() -> None:
     if not args.no_batch:
         batched = run_batched(ctx, lp, torch, stream, args.steps, max(1, min(args.warmup, 2)), args.batch_count)
 
+    serving = None
+    if not args.no_serve and world == 1:
+        serving = run_serving(lp, [float(r) for r in args.serve_rates.split(",")], args.serve_precisions.split(","))
+
     # ---- end to end through the C ABI with pinned host buffers ----
     e2e = None
     if not args.no_e2e:
@@ -460,6 +500,8 @@ def main() -> None:
         line["mixed"] = mixed
     if batched is not None:
         line["batched"] = batched
+    if serving is not None:
+        line["serving"] = serving
     if e2e is not None:
         line["e2e"] = e2e
     if world == 1 and not args.no_cpu:

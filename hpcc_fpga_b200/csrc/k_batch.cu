@@ -32,6 +32,9 @@ constexpr int SMALL_MAX = 128;
 constexpr int RHS_MAX = 16;
 constexpr int TILE = 64;
 constexpr int NBUCKETS = 5;
+// Flag in BatchSys::nrhs (server use only; the public entry points accept
+// nrhs <= 16): the matrix already holds its factors, solve only.
+constexpr int kSolveOnly = kBatchSolveOnly;
 
 struct BatchSys {
     int n, nrhs, lda, ldb;
@@ -42,6 +45,7 @@ static_assert(sizeof(BatchSys) == sizeof(lp_system), "lp_system layout");
 struct Tune {
     int small_n_max;
     int nb[NBUCKETS];
+    int absolute;  // a_off / b_off are device addresses (bytes), not offsets into A / B
 };
 
 constexpr size_t kSmallFloats = (size_t)SMALL_MAX * (SMALL_MAX + 1) + (size_t)RHS_MAX * SMALL_MAX;
@@ -105,7 +109,7 @@ __device__ void smem_solve(const float* S, int ld, int m, float* Y, int nrhs, fl
     }
 }
 
-__device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
+__device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrhs, bool factor, float* sm) {
     const int ld = n | 1;  // odd stride: column reads hit distinct banks
     float* S = sm;
     float* Y = sm + SMALL_MAX * (SMALL_MAX + 1);
@@ -119,12 +123,13 @@ __device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrh
         Y[idx] = b[(size_t)q * ldb + i];
     }
     __syncthreads();
-    smem_lu(S, ld, n);
+    if (factor) smem_lu(S, ld, n);
     smem_solve(S, ld, n, Y, nrhs, sc);
-    for (int idx = threadIdx.x; idx < n * n; idx += BT) {
-        const int r = idx / n, c = idx - r * n;
-        a[(size_t)r * lda + c] = S[r * ld + c];
-    }
+    if (factor)
+        for (int idx = threadIdx.x; idx < n * n; idx += BT) {
+            const int r = idx / n, c = idx - r * n;
+            a[(size_t)r * lda + c] = S[r * ld + c];
+        }
     for (int idx = threadIdx.x; idx < nrhs * n; idx += BT) {
         const int q = idx / n, i = idx - q * n;
         b[(size_t)q * ldb + i] = Y[idx];
@@ -342,16 +347,20 @@ __global__ void __launch_bounds__(BT, 2) k_batch_solve(const BatchSys* __restric
         __syncthreads();
         if (t >= count) break;
         const BatchSys s = sys[t];
-        float* a = A + s.a_off;
-        float* b = B + s.b_off;
+        float* a = tune.absolute ? reinterpret_cast<float*>(s.a_off) : A + s.a_off;
+        float* b = tune.absolute ? reinterpret_cast<float*>(s.b_off) : B + s.b_off;
+        const bool factor = (s.nrhs & kSolveOnly) == 0;
+        const int nrhs = s.nrhs & (kSolveOnly - 1);
         if (s.n <= tune.small_n_max) {
-            solve_small(a, s.lda, s.n, b, s.ldb, s.nrhs, sm);
+            solve_small(a, s.lda, s.n, b, s.ldb, nrhs, factor, sm);
         } else {
-            if (tune.nb[bucket_of(s.n)] == 16)
-                factor_blocked<16>(a, s.lda, s.n, sm);
-            else
-                factor_blocked<32>(a, s.lda, s.n, sm);
-            solve_blocked(a, s.lda, s.n, b, s.ldb, s.nrhs, sm);
+            if (factor) {
+                if (tune.nb[bucket_of(s.n)] == 16)
+                    factor_blocked<16>(a, s.lda, s.n, sm);
+                else
+                    factor_blocked<32>(a, s.lda, s.n, sm);
+            }
+            solve_blocked(a, s.lda, s.n, b, s.ldb, nrhs, sm);
         }
     }
 }
@@ -376,8 +385,10 @@ int validate_batch(int count, const lp_system* systems) {
 }
 
 int launch_batch(lp_ctx* c, const lp_system* d_sorted, int count, float* dA, float* dB, const lp_batch_config& cfg,
-                 int* d_next, cudaStream_t st) {
+                 int* d_next, cudaStream_t st, bool absolute) {
+    static_assert(kSolveOnly > RHS_MAX, "solve-only flag above the nrhs range");
     Tune tune;
+    tune.absolute = absolute ? 1 : 0;
     tune.small_n_max = cfg.small_n_max;
     for (int i = 0; i < NBUCKETS; i++) tune.nb[i] = cfg.nb[i];
     const int per_sm = cfg.ctas_per_sm < 1 ? 1 : (cfg.ctas_per_sm > 3 ? 3 : cfg.ctas_per_sm);

@@ -1,15 +1,23 @@
-// lu stage: LU without pivoting of one diagonal block (bs <= 128), the block
-// resident in shared memory, one CTA.
+// lu stage: LU without pivoting of one diagonal block (16 <= bs <= 128), the
+// block resident in shared memory of one CTA.
 //
 // Arithmetic follows gefa_ref_nopvt (LINPACK/src/host/linpack_data.cpp:166-196)
 // operation for operation, with no fused multiply-add, so the block result is
 // bit-identical to the reference's host routine:
-//   d = -1/a_kk  (double division, rounded to float)
+//   d = -1/a_kk   (the reference divides in double and rounds to float; with
+//                  53 >= 2*24 + 2 bits that double rounding equals the
+//                  correctly rounded float reciprocal, __frcp_rn, negated)
 //   a_ki = a_ki * d                       (i > k)
 //   a_ji = a_ji + a_ki * a_jk             (j > k, i > k)
-// The scaled pivot row is not stored before the update: every thread forms
-// a_ki * d itself (same rounding), and row k is written back during step k+1,
-// when no thread reads it any more.  One barrier per step.
+//
+// Schedule: 32-wide chunks.  For the chunk at k0 the same operations are
+// grouped as (1) the 32 x 32 diagonal block, one warp, its columns across the
+// lanes; (2) the block row right of it (column-independent: each lane one
+// column) and the block column below it (row-independent: each lane one row),
+// concurrently on different warps; (3) the trailing update, every element
+// receiving its 32 updates in ascending k with a separate multiply and add.
+// Every element still sees exactly the reference's sequence of operations;
+// only independent operations are reordered.  Three barriers per chunk.
 #include "lp_common.cuh"
 
 namespace lp {
@@ -17,71 +25,149 @@ namespace {
 
 constexpr int kLuThreads = 512;
 
-__global__ void __launch_bounds__(kLuThreads) k_lu_small(float* __restrict__ a, int lda, int bs, int log2bs) {
-    extern __shared__ float s[];  // bs x bs, row-major
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    constexpr int nw = kLuThreads / 32;
-
-    for (int idx = tid; idx < bs * bs; idx += kLuThreads) {
-        const int r = idx >> log2bs, c = idx & (bs - 1);
-        s[idx] = a[(size_t)r * lda + c];
+// (1) In-place LU of the NB x NB block at D (row stride SL), one warp; lane c
+// holds column c (x[j] = D[j][c]).  Kept out of line: inlined into the chunk
+// loop, its register array is not fully unrolled and lands in local memory.
+template <int NB, int SL>
+__device__ __noinline__ void diag_lu(float* D, int lane) {
+    float x[NB];
+    const bool act = lane < NB;
+#pragma unroll
+    for (int j = 0; j < NB; j++) x[j] = act ? D[j * SL + lane] : 0.0f;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+        const float d = -__frcp_rn(__shfl_sync(0xffffffffu, x[k], k));
+        if (lane > k)
+            x[k] = __fmul_rn(x[k], d);  // scaled row k: the multipliers
+        else if (lane == k)
+            x[k] = d;
+#pragma unroll
+        for (int j = k + 1; j < NB; j++) {
+            const float sjk = __shfl_sync(0xffffffffu, x[j], k);  // column k, row j
+            if (lane > k) x[j] = __fadd_rn(x[j], __fmul_rn(x[k], sjk));
+        }
     }
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < NB; j++) D[j * SL + lane] = x[j];
+    }
+}
+
+// (2a) Column `col` of the block row right of the diagonal block at k0:
+// for k: t_k *= D_kk; t_j += t_k D_jk (j > k).
+template <int NB, int SL>
+__device__ __forceinline__ void top_column(float* S, int k0, int col) {
+    float x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; j++) x[j] = S[(k0 + j) * SL + col];
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+        x[k] = __fmul_rn(x[k], S[(k0 + k) * SL + k0 + k]);
+#pragma unroll
+        for (int j = k + 1; j < NB; j++) x[j] = __fadd_rn(x[j], __fmul_rn(x[k], S[(k0 + j) * SL + k0 + k]));
+    }
+#pragma unroll
+    for (int j = 0; j < NB; j++) S[(k0 + j) * SL + col] = x[j];
+}
+
+// (2b) Row `row` of the block column below the diagonal block at k0:
+// for k, i > k: l_i += l_k D_ki.
+template <int NB, int SL>
+__device__ __forceinline__ void left_row(float* S, int k0, int row) {
+    float x[NB];
+#pragma unroll
+    for (int i = 0; i < NB; i++) x[i] = S[row * SL + k0 + i];
+#pragma unroll
+    for (int k = 0; k < NB; k++)
+#pragma unroll
+        for (int i = k + 1; i < NB; i++) x[i] = __fadd_rn(x[i], __fmul_rn(x[k], S[(k0 + k) * SL + k0 + i]));
+#pragma unroll
+    for (int i = 0; i < NB; i++) S[row * SL + k0 + i] = x[i];
+}
+
+template <int BS>
+__global__ void __launch_bounds__(kLuThreads) k_lu_block(float* __restrict__ a, int lda) {
+    constexpr int NB = BS < 32 ? BS : 32;
+    constexpr int SL = BS + 4;  // 16-byte rows
+    extern __shared__ __align__(16) float S[];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int idx = tid; idx < BS * BS; idx += kLuThreads) {
+        const int r = idx / BS, c = idx - r * BS;
+        cp_async4(S + r * SL + c, a + (size_t)r * lda + c);
+    }
+    cp_async_wait_all();
     __syncthreads();
 
-    float inv_prev = 0.0f;
-    for (int k = 0; k < bs; k++) {
-        const float inv = (float)(-1.0 / (double)s[k * bs + k]);
-        // Finalize the previous pivot row: store -1/d and the scaled row.
-        if (k > 0) {
-            float* rp = s + (k - 1) * bs;
-            for (int i = k + tid; i < bs; i += kLuThreads) rp[i] = __fmul_rn(rp[i], inv_prev);
-            if (tid == 0) rp[k - 1] = inv_prev;
-        }
-        // Rank-1 update of the trailing part with the (on-the-fly scaled) row k.
-        const float* rk = s + k * bs;
-        float sc[4];
-        int ii[4];
+    for (int k0 = 0; k0 < BS; k0 += NB) {
+        if (warp == 0) diag_lu<NB, SL>(S + k0 * SL + k0, lane);
+        __syncthreads();
+        const int base = k0 + NB, rest = BS - base;  // a multiple of 32
+        if (rest == 0) break;
+        if (warp < rest / 32)
+            top_column<NB, SL>(S, k0, base + 32 * warp + lane);
+        else if (warp >= 8 && warp - 8 < rest / 32)
+            left_row<NB, SL>(S, k0, base + 32 * (warp - 8) + lane);
+        __syncthreads();
+        // (3) trailing update: rows / columns [base, BS); lane = column, warp = row (two rows per pass)
+        for (int g = 0; g < rest / 32; g++) {
+            const int i = base + 32 * g + lane;
+            float tv[NB];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            ii[q] = k + 1 + lane + 32 * q;
-            sc[q] = (ii[q] < bs) ? __fmul_rn(rk[ii[q]], inv) : 0.0f;
-        }
-        for (int j = k + 1 + warp; j < bs; j += nw) {
-            float* rj = s + j * bs;
-            const float sjk = rj[k];
+            for (int kk = 0; kk < NB; kk++) tv[kk] = S[(k0 + kk) * SL + i];
+            for (int r = base + warp; r < BS; r += 32) {
+                const int r2 = r + 16;  // rest / 16 is even
+                float acc = S[r * SL + i], acc2 = S[r2 * SL + i];
+                const float* l1 = S + r * SL + k0;
+                const float* l2 = S + r2 * SL + k0;
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                if (ii[q] < bs) rj[ii[q]] = __fadd_rn(rj[ii[q]], __fmul_rn(sc[q], sjk));
+                for (int kk = 0; kk < NB; kk += 4) {
+                    const float4 u = *reinterpret_cast<const float4*>(l1 + kk);
+                    const float4 v = *reinterpret_cast<const float4*>(l2 + kk);
+                    acc = __fadd_rn(acc, __fmul_rn(tv[kk], u.x));
+                    acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk], v.x));
+                    acc = __fadd_rn(acc, __fmul_rn(tv[kk + 1], u.y));
+                    acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 1], v.y));
+                    acc = __fadd_rn(acc, __fmul_rn(tv[kk + 2], u.z));
+                    acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 2], v.z));
+                    acc = __fadd_rn(acc, __fmul_rn(tv[kk + 3], u.w));
+                    acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 3], v.w));
+                }
+                S[r * SL + i] = acc;
+                S[r2 * SL + i] = acc2;
+            }
         }
-        inv_prev = inv;
         __syncthreads();
     }
-    if (tid == 0) s[(bs - 1) * bs + (bs - 1)] = inv_prev;
-    __syncthreads();
 
-    for (int idx = tid; idx < bs * bs; idx += kLuThreads) {
-        const int r = idx >> log2bs, c = idx & (bs - 1);
-        a[(size_t)r * lda + c] = s[idx];
+    for (int idx = tid; idx < BS * BS; idx += kLuThreads) {
+        const int r = idx / BS, c = idx - r * BS;
+        a[(size_t)r * lda + c] = S[r * SL + c];
     }
+}
+
+template <int BS>
+constexpr size_t lu_smem() {
+    return sizeof(float) * (size_t)BS * (BS + 4);
 }
 
 }  // namespace
 
 int launch_lu_small(float* a, int lda, int bs, cudaStream_t st) {
-    if (!is_pow2(bs) || bs > 128 || bs < 1) return fail(LP_E_INVALID, "lu_small: bs must be a power of two <= 128");
-    int log2bs = 0;
-    while ((1 << log2bs) < bs) log2bs++;
-    const size_t smem = sizeof(float) * (size_t)bs * bs;
-    k_lu_small<<<1, kLuThreads, smem, st>>>(a, lda, bs, log2bs);
+    switch (bs) {
+        case 16: k_lu_block<16><<<1, kLuThreads, lu_smem<16>(), st>>>(a, lda); break;
+        case 32: k_lu_block<32><<<1, kLuThreads, lu_smem<32>(), st>>>(a, lda); break;
+        case 64: k_lu_block<64><<<1, kLuThreads, lu_smem<64>(), st>>>(a, lda); break;
+        case 128: k_lu_block<128><<<1, kLuThreads, lu_smem<128>(), st>>>(a, lda); break;
+        default: return fail(LP_E_INVALID, "lu block: bs must be 16, 32, 64 or 128");
+    }
     count_launch();
     LP_CUDA(cudaGetLastError());
     return LP_OK;
 }
 
 int lu_init_attrs() {
-    LP_CUDA(cudaFuncSetAttribute(k_lu_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 128 * 4));
+    LP_CUDA(cudaFuncSetAttribute(k_lu_block<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_lu_block<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lu_smem<64>()));
     return LP_OK;
 }
 

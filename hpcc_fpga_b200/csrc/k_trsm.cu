@@ -145,6 +145,180 @@ __global__ void __launch_bounds__(kTrsmThreads) k_trsm_left(const float* __restr
     }
 }
 
+// ---- bs <= 128: 32-wide chunks, each recurrence lane-parallel ----------
+// The diagonal block and the CTA's 32 columns (top) or rows (left) sit in
+// shared memory.  Per 32-wide chunk: one warp runs the recurrence of the
+// chunk with one independent column (top) / row (left) per lane, then all
+// warps apply the finished chunk to the remaining rows (top) / columns (left),
+// every element receiving its 32 updates in ascending k with a separate
+// multiply and add.  Same per-element operation sequence as above.
+constexpr int kCW = 32;  // columns (top) / rows (left) per CTA
+
+template <int BS>
+__global__ void __launch_bounds__(kTrsmThreads) k_top_chunk(const float* __restrict__ lu, int ldlu,
+                                                          float* __restrict__ t, int ldt, int ncols) {
+    constexpr int NB = BS < 32 ? BS : 32;
+    constexpr int SL = BS + 4, TL = kCW + 4;
+    extern __shared__ __align__(16) float sm[];
+    float* D = sm;             // BS x SL: the factored diagonal block
+    float* T = sm + BS * SL;   // BS x TL: the CTA's columns
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c0 = blockIdx.x * kCW;
+    for (int idx = tid; idx < BS * BS; idx += kTrsmThreads) {
+        const int j = idx / BS, k = idx - j * BS;
+        cp_async4(D + j * SL + k, lu + (size_t)j * ldlu + k);
+    }
+    for (int idx = tid; idx < BS * kCW; idx += kTrsmThreads) {
+        const int r = idx / kCW, cc = idx - r * kCW;
+        if (c0 + cc < ncols)
+            cp_async4(T + r * TL + cc, t + (size_t)r * ldt + c0 + cc);
+        else
+            T[r * TL + cc] = 0.0f;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int k0 = 0; k0 < BS; k0 += NB) {
+        if (warp == 0) {  // rows k0..k0+NB-1 of column `lane`: t_k *= D_kk; t_j += t_k D_jk
+            float x[NB];
+#pragma unroll
+            for (int j = 0; j < NB; j++) x[j] = T[(k0 + j) * TL + lane];
+#pragma unroll
+            for (int k = 0; k < NB; k++) {
+                x[k] = __fmul_rn(x[k], D[(k0 + k) * SL + k0 + k]);
+#pragma unroll
+                for (int j = k + 1; j < NB; j++)
+                    x[j] = __fadd_rn(x[j], __fmul_rn(x[k], D[(k0 + j) * SL + k0 + k]));
+            }
+#pragma unroll
+            for (int j = 0; j < NB; j++) T[(k0 + j) * TL + lane] = x[j];
+        }
+        __syncthreads();
+        const int base = k0 + NB;
+        if (base == BS) break;
+        // rows below the chunk: T[r][c] += sum_kk T[k0+kk][c] D[r][k0+kk]; two rows per pass
+        float tv[NB];
+#pragma unroll
+        for (int kk = 0; kk < NB; kk++) tv[kk] = T[(k0 + kk) * TL + lane];
+        for (int r = base + warp; r < BS; r += 16) {
+            const int r2 = r + 8;  // (BS - base) / 8 is even
+            float acc = T[r * TL + lane], acc2 = T[r2 * TL + lane];
+            const float* d1 = D + r * SL + k0;
+            const float* d2 = D + r2 * SL + k0;
+#pragma unroll
+            for (int kk = 0; kk < NB; kk += 4) {
+                const float4 u = *reinterpret_cast<const float4*>(d1 + kk);
+                const float4 v = *reinterpret_cast<const float4*>(d2 + kk);
+                acc = __fadd_rn(acc, __fmul_rn(tv[kk], u.x));
+                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk], v.x));
+                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 1], u.y));
+                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 1], v.y));
+                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 2], u.z));
+                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 2], v.z));
+                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 3], u.w));
+                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 3], v.w));
+            }
+            T[r * TL + lane] = acc;
+            T[r2 * TL + lane] = acc2;
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < BS * kCW; idx += kTrsmThreads) {
+        const int r = idx / kCW, cc = idx - r * kCW;
+        if (c0 + cc < ncols) t[(size_t)r * ldt + c0 + cc] = T[r * TL + cc];
+    }
+}
+
+template <int BS>
+__global__ void __launch_bounds__(kTrsmThreads) k_left_chunk(const float* __restrict__ lu, int ldlu,
+                                                           float* __restrict__ l, int ldl, int nrows,
+                                                           float* __restrict__ lt, int ldlt) {
+    constexpr int NB = BS < 32 ? BS : 32;
+    constexpr int SL = BS + 4;
+    extern __shared__ __align__(16) float sm[];
+    float* D = sm;             // BS x SL: the factored diagonal block
+    float* L = sm + BS * SL;   // kCW x SL: the CTA's rows
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int r0 = blockIdx.x * kCW;
+    for (int idx = tid; idx < BS * BS; idx += kTrsmThreads) {
+        const int k = idx / BS, i = idx - k * BS;
+        cp_async4(D + k * SL + i, lu + (size_t)k * ldlu + i);
+    }
+    for (int idx = tid; idx < kCW * BS; idx += kTrsmThreads) {
+        const int r = idx / BS, c = idx - r * BS;
+        if (r0 + r < nrows)
+            cp_async4(L + r * SL + c, l + (size_t)(r0 + r) * ldl + c);
+        else
+            L[r * SL + c] = 0.0f;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int k0 = 0; k0 < BS; k0 += NB) {
+        if (warp == 0) {  // columns k0..k0+NB-1 of row `lane`: l_i += l_k D_ki (i > k)
+            float x[NB];
+#pragma unroll
+            for (int i = 0; i < NB; i++) x[i] = L[lane * SL + k0 + i];
+#pragma unroll
+            for (int k = 0; k < NB; k++)
+#pragma unroll
+                for (int i = k + 1; i < NB; i++)
+                    x[i] = __fadd_rn(x[i], __fmul_rn(x[k], D[(k0 + k) * SL + k0 + i]));
+#pragma unroll
+            for (int i = 0; i < NB; i++) L[lane * SL + k0 + i] = x[i];
+        }
+        __syncthreads();
+        const int base = k0 + NB;
+        if (base == BS) break;
+        // columns after the chunk: L[r][i] += sum_kk L[r][k0+kk] D[k0+kk][i]; lane = column, warp = row
+        for (int g = 0; g < (BS - base) / 32; g++) {
+            const int i = base + 32 * g + lane;
+            float dv[NB];
+#pragma unroll
+            for (int kk = 0; kk < NB; kk++) dv[kk] = D[(k0 + kk) * SL + i];
+            float acc[kCW / 8];
+#pragma unroll
+            for (int s = 0; s < kCW / 8; s++) acc[s] = L[(warp + 8 * s) * SL + i];
+#pragma unroll
+            for (int kk = 0; kk < NB; kk += 4) {
+#pragma unroll
+                for (int s = 0; s < kCW / 8; s++) {
+                    const float4 u = *reinterpret_cast<const float4*>(L + (warp + 8 * s) * SL + k0 + kk);
+                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.x, dv[kk]));
+                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.y, dv[kk + 1]));
+                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.z, dv[kk + 2]));
+                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.w, dv[kk + 3]));
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < kCW / 8; s++) L[(warp + 8 * s) * SL + i] = acc[s];
+        }
+        __syncthreads();
+    }
+    for (int idx = tid; idx < kCW * BS; idx += kTrsmThreads) {
+        const int r = idx / BS, c = idx - r * BS;
+        if (r0 + r < nrows) l[(size_t)(r0 + r) * ldl + c] = L[r * SL + c];
+    }
+    if (lt == nullptr) return;
+    for (int idx = tid; idx < kCW * BS; idx += kTrsmThreads) {
+        const int c = idx / kCW, r = idx - c * kCW;
+        if (r0 + r < nrows) lt[(size_t)c * ldlt + r0 + r] = L[r * SL + c];
+    }
+}
+
+template <int BS>
+constexpr size_t top_chunk_smem() { return sizeof(float) * ((size_t)BS * (BS + 4) + (size_t)BS * (kCW + 4)); }
+template <int BS>
+constexpr size_t left_chunk_smem() { return sizeof(float) * ((size_t)BS * (BS + 4) + (size_t)kCW * (BS + 4)); }
+
+template <int BS>
+void launch_left_chunk(const float* lu, int ldlu, float* l, int ldl, int nrows, float* lt, int ldlt, cudaStream_t st) {
+    k_left_chunk<BS><<<(nrows + kCW - 1) / kCW, kTrsmThreads, left_chunk_smem<BS>(), st>>>(lu, ldlu, l, ldl, nrows,
+                                                                                          lt, ldlt);
+}
+template <int BS>
+void launch_top_chunk(const float* lu, int ldlu, float* t, int ldt, int ncols, cudaStream_t st) {
+    k_top_chunk<BS><<<(ncols + kCW - 1) / kCW, kTrsmThreads, top_chunk_smem<BS>(), st>>>(lu, ldlu, t, ldt, ncols);
+}
+
 int log2i(int x) {
     int r = 0;
     while ((1 << r) < x) r++;
@@ -162,6 +336,10 @@ int trsm_init_attrs() {
     LP_CUDA(cudaFuncSetAttribute(k_trsm_top<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)top_smem(512, 16)));
     LP_CUDA(cudaFuncSetAttribute(k_trsm_left<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
     LP_CUDA(cudaFuncSetAttribute(k_trsm_left<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)left_smem(512, 16)));
+    LP_CUDA(cudaFuncSetAttribute(k_left_chunk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)left_chunk_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_top_chunk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)top_chunk_smem<128>()));
     return LP_OK;
 }
 
@@ -169,7 +347,16 @@ int launch_trsm_top(const float* lu, int ldlu, float* t, int ldt, int bs, int nc
     if (!is_pow2(bs) || bs < 16 || bs > 512) return fail(LP_E_INVALID, "top_update: bs must be a power of two in [16, 512]");
     if (ncols <= 0) return LP_OK;
     const dim3 grid((ncols + kStrip - 1) / kStrip);
-    if (bs >= 32)
+    if (bs <= 128) {
+        if (bs == 128)
+            launch_top_chunk<128>(lu, ldlu, t, ldt, ncols, st);
+        else if (bs == 64)
+            launch_top_chunk<64>(lu, ldlu, t, ldt, ncols, st);
+        else if (bs == 32)
+            launch_top_chunk<32>(lu, ldlu, t, ldt, ncols, st);
+        else
+            launch_top_chunk<16>(lu, ldlu, t, ldt, ncols, st);
+    } else if (bs >= 32)
         k_trsm_top<32><<<grid, kTrsmThreads, top_smem(bs, 32), st>>>(lu, ldlu, t, ldt, bs, ncols);
     else
         k_trsm_top<16><<<grid, kTrsmThreads, top_smem(bs, 16), st>>>(lu, ldlu, t, ldt, bs, ncols);
@@ -184,7 +371,16 @@ int launch_trsm_left(const float* lu, int ldlu, float* l, int ldl, int bs, int n
     if (nrows <= 0) return LP_OK;
     const dim3 grid((nrows + kStrip - 1) / kStrip);
     const int lg = log2i(bs);
-    if (bs >= 32)
+    if (bs <= 128) {
+        if (bs == 128)
+            launch_left_chunk<128>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+        else if (bs == 64)
+            launch_left_chunk<64>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+        else if (bs == 32)
+            launch_left_chunk<32>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+        else
+            launch_left_chunk<16>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+    } else if (bs >= 32)
         k_trsm_left<32><<<grid, kTrsmThreads, left_smem(bs, 32), st>>>(lu, ldlu, l, ldl, bs, lg, nrows, lt, ldlt);
     else
         k_trsm_left<16><<<grid, kTrsmThreads, left_smem(bs, 16), st>>>(lu, ldlu, l, ldl, bs, lg, nrows, lt, ldlt);

@@ -10,10 +10,6 @@
 
 namespace lp {
 
-int validate_batch(int count, const lp_system* systems);
-int launch_batch(lp_ctx* c, const lp_system* d_sorted, int count, float* dA, float* dB, const lp_batch_config& cfg,
-                 int* d_next, cudaStream_t st);
-
 namespace {
 
 uint64_t fnv(const void* p, size_t bytes, uint64_t h = 1469598103934665603ull) {

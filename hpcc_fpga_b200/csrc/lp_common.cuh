@@ -33,6 +33,16 @@ void count_launch(long long n = 1);
 long long launch_count();
 inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
 
+#ifdef __CUDACC__
+// 4-byte asynchronous global -> shared copy (any float address), and the wait
+// for all of the calling thread's outstanding copies.
+__device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+#endif
+
 // ---- kernel launchers (each returns LP_OK or an error status) ------------
 // Diagonal block LU for bs <= 128, whole block in shared memory.
 int launch_lu_small(float* a, int lda, int bs, cudaStream_t s);

@@ -34,6 +34,13 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
                        cudaStream_t st);
 int umma_init_attrs();
 int batch_init_attrs();
+int validate_batch(int count, const lp_system* systems);
+// One persistent batched launch over d_sorted (device descriptors, largest n
+// first).  absolute: a_off / b_off are device addresses instead of offsets
+// into dA / dB; nrhs may then carry the solve-only flag (factors present).
+int launch_batch(lp_ctx* c, const lp_system* d_sorted, int count, float* dA, float* dB, const lp_batch_config& cfg,
+                 int* d_next, cudaStream_t st, bool absolute = false);
+constexpr int kBatchSolveOnly = 1 << 8;
 // x = LU \ b, then FP64 refinement against the original matrix a0 until the
 // HPL scaled residual is <= 16 or max_iters refinements were made.
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,

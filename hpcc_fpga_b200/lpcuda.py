@@ -80,6 +80,43 @@ class LpBatchStats(ctypes.Structure):
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
 
 
+LP_SERVE_CONTINUOUS, LP_SERVE_PER_REQUEST = 0, 1
+
+
+class LpServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("mode", ctypes.c_int), ("precision", ctypes.c_int),
+                ("slots", ctypes.c_int), ("batch_workers", ctypes.c_int), ("batch_max_n", ctypes.c_int),
+                ("batch_max_count", ctypes.c_int), ("max_refinements", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class LpRequest(ctypes.Structure):
+    _fields_ = [("key", ctypes.c_longlong), ("n", ctypes.c_int), ("nrhs", ctypes.c_int), ("A", _VP),
+                ("lda", ctypes.c_int), ("B", _VP), ("ldb", ctypes.c_int), ("X", _VP), ("ldx", ctypes.c_int)]
+
+
+class LpResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_longlong), ("key", ctypes.c_longlong), ("status", ctypes.c_int),
+                ("n", ctypes.c_int), ("nrhs", ctypes.c_int), ("reused", ctypes.c_int), ("batched", ctypes.c_int),
+                ("ir_iters", ctypes.c_int), ("hpl_resid", ctypes.c_double), ("t_submit", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
+class LpServerInfo(ctypes.Structure):
+    _fields_ = [("pending", ctypes.c_int), ("running", ctypes.c_int), ("resident", ctypes.c_int),
+                ("used_bytes", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("waves", ctypes.c_longlong),
+                ("waved_systems", ctypes.c_longlong), ("evictions", ctypes.c_longlong),
+                ("rejected", ctypes.c_longlong)]
+
+    def as_dict(self) -> dict:
+        return {f[0]: getattr(self, f[0]) for f in self._fields_}
+
+
 class LpError(RuntimeError):
     def __init__(self, status: int, where: str, detail: str):
         self.status = status
@@ -131,6 +168,13 @@ def lib() -> ctypes.CDLL:
     L.lp_generate_reference.argtypes = [_F32P, _F32P, _I, _I, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float)]
     L.lp_generate_baseline.argtypes = [_F32P, _VP, _VP, _I, ctypes.c_uint, ctypes.c_double]
+    L.lp_server_default_config.argtypes = [ctypes.POINTER(LpServerConfig)]
+    L.lp_server_start.argtypes = [_I, ctypes.POINTER(LpServerConfig), ctypes.POINTER(_VP)]
+    L.lp_server_stop.argtypes = [_VP]
+    L.lp_server_submit.argtypes = [_VP, ctypes.POINTER(LpRequest), ctypes.POINTER(ctypes.c_longlong)]
+    L.lp_server_poll.argtypes = [_VP, ctypes.POINTER(LpResult), _I, _I, ctypes.POINTER(_I)]
+    L.lp_server_get_info.argtypes = [_VP, ctypes.POINTER(LpServerInfo)]
+    L.lp_server_replay.argtypes = [_VP, _I, ctypes.POINTER(LpRequest), _F64P, ctypes.POINTER(LpResult), _I]
     _lib = L
     return L
 
@@ -307,3 +351,115 @@ class Context:
         check(lib().lp_solve_host(self._h, PRECISIONS[precision], n, bs, A, A.shape[1], B, nrhs, x, max_iters,
                                   ctypes.byref(t)), "lp_solve_host")
         return (x[0] if np.ndim(b64) == 1 else x), t.as_dict()
+
+
+# ------------------------------------------------------------------ pinned host memory
+class Pinned:
+    """Page-locked host buffer (lp_host_alloc) viewed as a numpy array."""
+
+    def __init__(self, shape, dtype=np.float32):
+        dtype = np.dtype(dtype)
+        count = int(np.prod(shape))
+        p = _VP()
+        check(lib().lp_host_alloc(ctypes.c_size_t(max(1, count) * dtype.itemsize), ctypes.byref(p)),
+              "lp_host_alloc")
+        self._p = p
+        buf = (ctypes.c_char * (max(1, count) * dtype.itemsize)).from_address(p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=count).reshape(shape)
+
+    @property
+    def ptr(self) -> int:
+        return self._p.value
+
+    def free(self) -> None:
+        if self._p:
+            self.array = None
+            lib().lp_host_free(self._p)
+            self._p = _VP()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ serving loop
+def server_config(**kw) -> LpServerConfig:
+    """Default lp_server_config with fields overridden by keyword (precision
+    may be given as "f32" / "bf16" / "fp8", mode as "continuous" / "per_request")."""
+    cfg = LpServerConfig()
+    check(lib().lp_server_default_config(ctypes.byref(cfg)), "lp_server_default_config")
+    for k, v in kw.items():
+        if k == "precision" and isinstance(v, str):
+            v = PRECISIONS[v]
+        if k == "mode" and isinstance(v, str):
+            v = {"continuous": LP_SERVE_CONTINUOUS, "per_request": LP_SERVE_PER_REQUEST}[v]
+        setattr(cfg, k, int(v))
+    return cfg
+
+
+class Server:
+    """lp_server: asynchronous solve requests with resident factors."""
+
+    def __init__(self, device: int = 0, cfg: LpServerConfig | None = None, **kw):
+        if cfg is None:
+            cfg = server_config(**kw)
+        h = _VP()
+        check(lib().lp_server_start(device, ctypes.byref(cfg), ctypes.byref(h)), "lp_server_start")
+        self._h = h
+        self.cfg = cfg
+
+    def stop(self) -> None:
+        if self._h:
+            lib().lp_server_stop(self._h)
+            self._h = _VP()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
+
+    def submit(self, req: LpRequest) -> int:
+        rid = ctypes.c_longlong()
+        check(lib().lp_server_submit(self._h, ctypes.byref(req), ctypes.byref(rid)), "lp_server_submit")
+        return rid.value
+
+    def poll(self, max_results: int = 256, timeout_ms: int = 1000) -> list[dict]:
+        """Finished results (possibly none when the wait times out)."""
+        out = (LpResult * max_results)()
+        k = _I(0)
+        st = lib().lp_server_poll(self._h, out, max_results, timeout_ms, ctypes.byref(k))
+        if st not in (LP_OK, LP_E_TIMEOUT):
+            check(st, "lp_server_poll")
+        return [out[i].as_dict() for i in range(k.value)]
+
+    def wait(self, count: int, timeout_ms: int = 60000) -> list[dict]:
+        """Poll until `count` results arrived; LpError(LP_E_TIMEOUT) if a wait expires."""
+        got: list[dict] = []
+        while len(got) < count:
+            out = (LpResult * 256)()
+            k = _I(0)
+            check(lib().lp_server_poll(self._h, out, 256, timeout_ms, ctypes.byref(k)), "lp_server_poll")
+            got += [out[i].as_dict() for i in range(k.value)]
+        return got
+
+    def info(self) -> dict:
+        i = LpServerInfo()
+        check(lib().lp_server_get_info(self._h, ctypes.byref(i)), "lp_server_get_info")
+        return i.as_dict()
+
+    def replay(self, reqs, arrival_s: np.ndarray, timeout_ms: int = 60000) -> list[dict]:
+        """Submit reqs[i] at arrival_s[i] (seconds from the call) and collect all results, in order."""
+        arr = (LpRequest * len(reqs))(*reqs)
+        out = (LpResult * len(reqs))()
+        t = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        check(lib().lp_server_replay(self._h, len(reqs), arr, t, out, timeout_ms), "lp_server_replay")
+        return [out[i].as_dict() for i in range(len(reqs))]

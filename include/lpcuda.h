@@ -244,6 +244,84 @@ int lp_batch_solve_dev(lp_ctx* ctx, int count, const lp_system* systems, float* 
 int lp_batch_autotune(lp_ctx* ctx, int count, const lp_system* systems, const float* dA, const float* dB,
                       lp_batch_config* out);
 
+/* ---- serving loop (addition: no counterpart in the reference) -------------
+ * A request loop on one GPU.  Requests (one diagonally dominant system,
+ * 1 <= n <= 16384, 1..16 right-hand sides) are submitted at any time and
+ * complete asynchronously (lp_server_poll).  In LP_SERVE_CONTINUOUS mode,
+ * requests that arrive while others are on the GPU are admitted as worker
+ * slots and device memory free up: systems with n <= batch_max_n gather into
+ * waves of the batched kernel (one persistent launch per wave, new
+ * factorizations and solves with resident factors side by side), larger ones
+ * run on `slots` concurrent streams.  LP_SERVE_PER_REQUEST is the baseline:
+ * one request at a time, each with the plain single-system launches.
+ * Factors stay resident, keyed by the caller's matrix key, so a later request
+ * with the same key and n only solves.  All device memory of the cache and
+ * of in-flight requests is charged against hbm_budget_bytes; idle factors
+ * are evicted least-recently-used first, a request that can never fit
+ * completes with LP_E_BUDGET.  Host buffers should be pinned (lp_host_alloc)
+ * so copies overlap; they must stay valid until the request completes. */
+#define LP_SERVE_CONTINUOUS 0
+#define LP_SERVE_PER_REQUEST 1
+typedef struct lp_server lp_server;
+typedef struct {
+    long long hbm_budget_bytes; /* device memory for resident factors + in-flight work (default 80e9) */
+    int mode;                   /* LP_SERVE_CONTINUOUS or LP_SERVE_PER_REQUEST */
+    int precision;              /* LP_F32, LP_BF16_IR or LP_FP8_IR */
+    int slots;                  /* concurrent large-system streams (1..16; 1 in per-request mode) */
+    int batch_workers;          /* concurrent waves of the batched kernel (1..4) */
+    int batch_max_n;            /* systems with n <= this (<= 1024) go to the batched kernel; 0: none */
+    int batch_max_count;        /* systems per wave */
+    int max_refinements;        /* FP64 refinement cap of the mixed precisions */
+} lp_server_config;
+typedef struct {
+    long long key;              /* matrix identity: same key and n reuse resident factors */
+    int n, nrhs;
+    const float* A;             /* n x n, leading dimension lda; may be NULL if the key is resident */
+    int lda;
+    const float* B;             /* nrhs right-hand sides as rows of ldb floats */
+    int ldb;
+    double* X;                  /* solutions, nrhs rows of ldx doubles */
+    int ldx;
+} lp_request;
+typedef struct {
+    long long id;               /* from lp_server_submit */
+    long long key;
+    int status;                 /* LP_OK or LP_E_* of this request */
+    int n, nrhs;
+    int reused;                 /* 1: resident factors were used */
+    int batched;                /* 1: served by a wave of the batched kernel */
+    int ir_iters;               /* FP64 refinements made */
+    double hpl_resid;           /* max over right-hand sides of ||b-Mx|| / ((||M|| ||x|| + ||b||) n eps), infinity
+                                   norms, eps = unit roundoff of the mode: FLT_EPSILON/2 for LP_F32,
+                                   DBL_EPSILON/2 for the refined precisions */
+    double t_submit, t_start, t_done; /* steady-clock seconds: submitted, work started, result written */
+} lp_result;
+typedef struct {
+    int pending;                /* submitted, not yet started */
+    int running;
+    int resident;               /* matrices with resident factors */
+    long long used_bytes;       /* charged against the budget */
+    long long completed, waves, waved_systems, evictions, rejected;
+} lp_server_info;
+int lp_server_default_config(lp_server_config* cfg);
+/* Starts the worker threads, each with its own context.  cfg NULL: default. */
+int lp_server_start(int device, const lp_server_config* cfg, lp_server** out);
+/* Waits for the running work, drops pending requests, frees everything. */
+int lp_server_stop(lp_server* s);
+/* Validates and queues one request (LP_E_INVALID for bad sizes or pointers,
+ * LP_E_STATE if A is NULL and the key is not resident). */
+int lp_server_submit(lp_server* s, const lp_request* req, long long* id);
+/* Copies up to max finished results into out (*count of them).  Waits up to
+ * timeout_ms for the first one; LP_E_TIMEOUT if none arrived. */
+int lp_server_poll(lp_server* s, lp_result* out, int max, int timeout_ms, int* count);
+int lp_server_get_info(lp_server* s, lp_server_info* info);
+/* Load replay: submits reqs[i] at arrival_s[i] seconds after the call (the
+ * calling thread keeps the schedule), collects every result into out[i], and
+ * returns when all completed; LP_E_TIMEOUT if no result arrived for
+ * timeout_ms.  Results must not be polled by another thread meanwhile. */
+int lp_server_replay(lp_server* s, int count, const lp_request* reqs, const double* arrival_s, lp_result* out,
+                     int timeout_ms);
+
 /* ---- input generation (host only, no GPU needed) ------------------------ */
 /* LinpackBenchmark::generateInputData for one rank
  * (LINPACK/src/host/linpack_benchmark.hpp:211-297): mt19937(0),
