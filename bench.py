@@ -249,6 +249,9 @@ def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
 FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
 
 
+RESERVE = 110 * 10 ** 9  # pool mapped at start: the 80 GB budget plus headroom against fragmentation
+
+
 def run_serving(lp, rates, precisions, master_n=8192) -> dict:
     """The serving workload: Poisson arrivals at each rate of the ladder, n
     log-uniform in [64, 8192], 1..16 right-hand sides, 30% of the requests
@@ -258,9 +261,6 @@ def run_serving(lp, rates, precisions, master_n=8192) -> dict:
     by the server's steady clock; solves/s over the first submission to the
     last completion of each replay."""
     from hpcc_fpga_b200 import serve
-
-    def count_for_rate(r):
-        return int(min(2000, max(300, 1.5 * r)))
 
     wl = serve.Workload(master_n=master_n, seed=42)
     out = {"workload": f"Poisson arrivals, n log-uniform in [64,{master_n}], 1-16 RHS, 30% reuse of one of the "
@@ -272,8 +272,9 @@ def run_serving(lp, rates, precisions, master_n=8192) -> dict:
             res = {}
             for mode in ("per_request", "continuous"):
                 t0 = time.perf_counter()
-                res[mode] = serve.ladder(lambda: lp.Server(0, precision=prec, mode=mode), wl, rates,
-                                         count_for_rate, seed=7)
+                res[mode] = serve.ladder(
+                    lambda: lp.Server(0, precision=prec, mode=mode, warm_n=master_n, reserve_bytes=RESERVE), wl,
+                    rates, seed=7)
                 res[mode + "_wall_s"] = round(time.perf_counter() - t0, 1)
             res["equal_p99"] = serve.equal_p99(res["per_request"], res["continuous"])
             out[prec] = res
@@ -330,7 +331,7 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
-    ap.add_argument("--serve-rates", default="100,300,1000,3000,10000,20000")
+    ap.add_argument("--serve-rates", default="100,200,300,400,500,600,700,800,900,1000,1250,1500,2000,5000,20000")
     ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
 

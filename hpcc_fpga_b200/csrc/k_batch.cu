@@ -13,11 +13,13 @@
 //     shared memory; right-looking LU with one barrier per step, then the
 //     forward and back sweeps.
 //   larger n: blocked right-looking LU with panel width NB (16 or 32, per
-//     size bucket, chosen by the autotuner): the diagonal block factored in
-//     shared memory; the top block row (column-independent) and left block
-//     column (row-independent) by their recurrences in registers; the
-//     trailing update as 64 x 64 register-tiled tiles through shared memory.
-//     (Panel widths 16 and 32 keep a column's recurrence in registers.)
+//     size bucket, chosen by the autotuner): the diagonal block factored by
+//     one warp in registers (pivots and columns by shuffles); the top block
+//     row (column-independent) and left block column (row-independent) by
+//     their recurrences in registers; the trailing update per 64-row block,
+//     its left panel resident in shared memory, the 64-column top tiles
+//     streamed through a cp.async double buffer and C accumulated in
+//     registers.  (Panel widths 16 and 32 keep a recurrence in registers.)
 //     Then blocked forward/back sweeps with the right-hand sides resident in
 //     shared memory and each diagonal block staged before its sequential solve.
 // Arithmetic uses fused multiply-add: results agree with the reference to
@@ -109,7 +111,7 @@ __device__ void smem_solve(const float* S, int ld, int m, float* Y, int nrhs, fl
     }
 }
 
-__device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrhs, bool factor, float* sm) {
+__device__ __noinline__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrhs, bool factor, float* sm) {
     const int ld = n | 1;  // odd stride: column reads hit distinct banks
     float* S = sm;
     float* Y = sm + SMALL_MAX * (SMALL_MAX + 1);
@@ -137,32 +139,62 @@ __device__ void solve_small(float* a, int lda, int n, float* b, int ldb, int nrh
     __syncthreads();
 }
 
+// LU of the kb x kb diagonal block at d (kb <= NB), warp 0 only: lane c
+// holds column c in registers, the pivot and column k are shuffled from lane
+// k.  Writes the factors to d and to Ds (row stride DL).  Out of line: inlined
+// into the persistent loop its register array is not fully unrolled.
+template <int NB, int DL>
+__device__ __noinline__ void warp_diag_lu(float* d, int lda, int kb, float* Ds) {
+    const int lane = threadIdx.x & 31;
+    const bool act = lane < kb;
+    float x[NB];
+#pragma unroll
+    for (int j = 0; j < NB; j++) x[j] = (act && j < kb) ? d[(size_t)j * lda + lane] : 0.0f;
+#pragma unroll
+    for (int k = 0; k < NB; k++) {
+        if (k < kb) {
+            const float inv = (float)(-1.0 / (double)__shfl_sync(0xffffffffu, x[k], k));
+            if (lane > k)
+                x[k] *= inv;
+            else if (lane == k)
+                x[k] = inv;
+#pragma unroll
+            for (int j = k + 1; j < NB; j++) {
+                if (j < kb) {
+                    const float sjk = __shfl_sync(0xffffffffu, x[j], k);
+                    if (lane > k) x[j] = fmaf(x[k], sjk, x[j]);
+                }
+            }
+        }
+    }
+    if (act) {
+#pragma unroll
+        for (int j = 0; j < NB; j++)
+            if (j < kb) {
+                d[(size_t)j * lda + lane] = x[j];
+                Ds[j * DL + lane] = x[j];
+            }
+    }
+}
+
 // Blocked factorization of one system in global memory (see file comment).
+// Trailing update per row block of TILE rows: the block's left panel (k-major)
+// stays in shared memory, the top tiles stream through a cp.async double
+// buffer, and each thread keeps its 4 x 4 piece of C in registers.
 template <int NB>
-__device__ void factor_blocked(float* a, int lda, int n, float* sm) {
-    constexpr int DL = NB + 1;
-    float* Ds = sm;                         // NB x (NB+1) diagonal block
-    float* Lt = Ds + NB * DL;               // NB x (TILE+1): left tile, k-major
-    float* Ts = Lt + NB * (TILE + 1);       // NB x TILE: top tile
+__device__ __noinline__ void factor_blocked(float* a, int lda, int n, float* sm) {
+    constexpr int DL = NB + 1, LS = TILE + 4;
+    float* Ds = sm;                    // NB x DL diagonal block
+    float* Lt = Ds + NB * DL;          // NB x LS: left panel of one row block, k-major
+    float* Tb = Lt + NB * LS;          // 2 x NB x TILE: top tiles
     const int tid = threadIdx.x;
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int kb = min(NB, n - k0);
         const int r0 = k0 + kb, rem = n - r0;
         float* d = a + (size_t)k0 * lda + k0;
-        for (int idx = tid; idx < kb * kb; idx += BT) {
-            const int r = idx / kb, c = idx - r * kb;
-            Ds[r * DL + c] = d[(size_t)r * lda + c];
-        }
+        if (tid < 32) warp_diag_lu<NB, DL>(d, lda, kb, Ds);
         __syncthreads();
-        smem_lu(Ds, DL, kb);
-        for (int idx = tid; idx < kb * kb; idx += BT) {
-            const int r = idx / kb, c = idx - r * kb;
-            d[(size_t)r * lda + c] = Ds[r * DL + c];
-        }
-        if (rem <= 0) {
-            __syncthreads();
-            break;
-        }
+        if (rem <= 0) break;
         // top: every column c of the block row, t_k *= D_kk; t_j += t_k D_jk (j > k)
         for (int c = r0 + tid; c < n; c += BT) {
             float x[NB];
@@ -196,52 +228,97 @@ __device__ void factor_blocked(float* a, int lda, int n, float* sm) {
                 if (i < kb) row[i] = x[i];
         }
         __syncthreads();
-        // inner: C[r0:n, r0:n] += L * T, 64 x 64 tiles, 4 x 4 per thread
+        // inner: C[r0:n, r0:n] += L * T
         const int ty = tid >> 4, tx = tid & 15;
         const int tiles = (rem + TILE - 1) / TILE;
-        for (int t = 0; t < tiles * tiles; t++) {
-            const int ti = t / tiles, tj = t - ti * tiles;
-            const int m0 = r0 + ti * TILE, c0 = r0 + tj * TILE;
-            for (int idx = tid; idx < TILE * kb; idx += BT) {
-                const int i = idx / kb, k = idx - i * kb;
-                Lt[k * (TILE + 1) + i] = (m0 + i < n) ? a[(size_t)(m0 + i) * lda + k0 + k] : 0.0f;
-            }
+        auto issue_top = [&](int tj, int buf) {
+            const int c0 = r0 + tj * TILE;
+            float* T = Tb + buf * (NB * TILE);
             for (int idx = tid; idx < kb * TILE; idx += BT) {
                 const int k = idx / TILE, j = idx - k * TILE;
-                Ts[k * TILE + j] = (c0 + j < n) ? a[(size_t)(k0 + k) * lda + c0 + j] : 0.0f;
+                if (c0 + j < n)
+                    cp_async4(T + k * TILE + j, a + (size_t)(k0 + k) * lda + c0 + j);
+                else
+                    T[k * TILE + j] = 0.0f;
             }
-            __syncthreads();
-            float acc[4][4];
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        };
+        const bool vec = ((lda & 3) == 0) && ((reinterpret_cast<uintptr_t>(a) & 15) == 0);
+        for (int ti = 0; ti < tiles; ti++) {
+            const int m0 = r0 + ti * TILE;
+            for (int idx = tid; idx < TILE * kb; idx += BT) {
+                const int i = idx / kb, k = idx - i * kb;
+                if (m0 + i < n)
+                    cp_async4(Lt + k * LS + i, a + (size_t)(m0 + i) * lda + k0 + k);
+                else
+                    Lt[k * LS + i] = 0.0f;
+            }
+            issue_top(0, 0);  // commits the left panel's copies with the first top tile
+            for (int tj = 0; tj < tiles; tj++) {
+                const int c0 = r0 + tj * TILE;
+                if (tj + 1 < tiles) issue_top(tj + 1, (tj + 1) & 1);
+                // this thread's 4 x 4 piece of C: loads in flight during the products
+                const int cc = c0 + tx * 4;
+                const bool full = vec && cc + 3 < n && ((cc & 3) == 0);
+                float cv[4][4];
 #pragma unroll
-            for (int p = 0; p < 4; p++)
+                for (int p = 0; p < 4; p++) {
+                    const int r = m0 + ty * 4 + p;
+                    if (r < n && full) {
+                        const float4 v = *reinterpret_cast<const float4*>(a + (size_t)r * lda + cc);
+                        cv[p][0] = v.x;
+                        cv[p][1] = v.y;
+                        cv[p][2] = v.z;
+                        cv[p][3] = v.w;
+                    } else {
 #pragma unroll
-                for (int q = 0; q < 4; q++) acc[p][q] = 0.0f;
-            for (int k = 0; k < kb; k++) {
-                const float* lrow = Lt + k * (TILE + 1) + ty * 4;
-                const float4 tv = *reinterpret_cast<const float4*>(Ts + k * TILE + tx * 4);
-                const float lv[4] = {lrow[0], lrow[1], lrow[2], lrow[3]};
-                const float tvv[4] = {tv.x, tv.y, tv.z, tv.w};
+                        for (int q = 0; q < 4; q++) cv[p][q] = (r < n && cc + q < n) ? a[(size_t)r * lda + cc + q] : 0.0f;
+                    }
+                }
+                if (tj + 1 < tiles)
+                    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+                else
+                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                __syncthreads();
+                const float* T = Tb + (tj & 1) * (NB * TILE);
+                float acc[4][4];
 #pragma unroll
                 for (int p = 0; p < 4; p++)
 #pragma unroll
-                    for (int q = 0; q < 4; q++) acc[p][q] = fmaf(lv[p], tvv[q], acc[p][q]);
-            }
+                    for (int q = 0; q < 4; q++) acc[p][q] = 0.0f;
+#pragma unroll 8
+                for (int k = 0; k < kb; k++) {
+                    const float4 lv = *reinterpret_cast<const float4*>(Lt + k * LS + ty * 4);
+                    const float4 tv = *reinterpret_cast<const float4*>(T + k * TILE + tx * 4);
+                    const float l4[4] = {lv.x, lv.y, lv.z, lv.w};
+                    const float t4[4] = {tv.x, tv.y, tv.z, tv.w};
 #pragma unroll
-            for (int p = 0; p < 4; p++) {
-                const int r = m0 + ty * 4 + p;
-                if (r >= n) continue;
-                float* crow = a + (size_t)r * lda + c0 + tx * 4;
+                    for (int p = 0; p < 4; p++)
 #pragma unroll
-                for (int q = 0; q < 4; q++)
-                    if (c0 + tx * 4 + q < n) crow[q] += acc[p][q];
+                        for (int q = 0; q < 4; q++) acc[p][q] = fmaf(l4[p], t4[q], acc[p][q]);
+                }
+#pragma unroll
+                for (int p = 0; p < 4; p++) {
+                    const int r = m0 + ty * 4 + p;
+                    if (r >= n) continue;
+                    if (full) {
+                        *reinterpret_cast<float4*>(a + (size_t)r * lda + cc) =
+                            make_float4(cv[p][0] + acc[p][0], cv[p][1] + acc[p][1], cv[p][2] + acc[p][2],
+                                        cv[p][3] + acc[p][3]);
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; q++)
+                            if (cc + q < n) a[(size_t)r * lda + cc + q] = cv[p][q] + acc[p][q];
+                    }
+                }
+                __syncthreads();  // this buffer is refilled two tiles later; Lt stays until the row block ends
             }
-            __syncthreads();
         }
     }
 }
 
 // Blocked forward/back sweeps, right-hand sides resident in shared memory.
-__device__ void solve_blocked(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
+__device__ __noinline__ void solve_blocked(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
     constexpr int SBK = 64, DL = SBK + 1;
     float* Y = sm;                       // nrhs x n
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;

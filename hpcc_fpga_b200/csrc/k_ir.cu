@@ -3,7 +3,8 @@
 //   residual  r = b - M x   with M = S^T, S the FP32 original matrix widened
 //             exactly to double, accumulated in double (gmres.c:190-191 does
 //             the same GEMV with dgemv_ref);
-//   norms     ||M||_inf (largest storage-column absolute sum), max |v|;
+//   norms     ||M||_inf (largest storage-column absolute sum), max |v| per
+//             right-hand side (reduced on the device, a few scalars copied back);
 //   update    x += d, and the FP64 -> FP32 narrowing of r for the low-
 //             precision solve.
 // The residual is a GEMV over storage rows: a CTA covers 256 unknowns
@@ -53,12 +54,18 @@ __global__ void __launch_bounds__(RT) k_colabs(const float* __restrict__ a, int 
     atomicAdd(&out[i], acc);
 }
 
-// out[0] = max |v| over n values (non-negative doubles compare as integers).
-__global__ void __launch_bounds__(RT) k_absmax(const double* __restrict__ v, size_t n, unsigned long long* out) {
+// out[q] = max |v[q*ld + i]| over i < n, for q = blockIdx.y; +infinity if any
+// value is not finite (non-negative doubles compare as their bit patterns).
+__global__ void __launch_bounds__(RT) k_rhs_absmax(const double* __restrict__ v, int n, int ld,
+                                                 unsigned long long* out) {
+    const double* vq = v + (size_t)blockIdx.y * ld;
     double m = 0.0;
-    for (size_t i = blockIdx.x * (size_t)RT + threadIdx.x; i < n; i += (size_t)gridDim.x * RT) m = fmax(m, fabs(v[i]));
+    for (int i = blockIdx.x * RT + threadIdx.x; i < n; i += gridDim.x * RT) {
+        const double a = vq[i];
+        m = isfinite(a) ? fmax(m, fabs(a)) : INFINITY;
+    }
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+    if ((threadIdx.x & 31) == 0) atomicMax(out + blockIdx.y, (unsigned long long)__double_as_longlong(m));
 }
 
 __global__ void k_axpy_f64(double* __restrict__ x, const float* __restrict__ d, size_t n) {
@@ -118,12 +125,12 @@ int launch_colabs(const float* a, int lda, int n, double* out, cudaStream_t st) 
     return LP_OK;
 }
 
-int launch_absmax(const double* v, size_t n, unsigned long long* out, cudaStream_t st) {
-    LP_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long), st));
-    int grid = (int)((n + RT - 1) / RT);
-    if (grid > 1184) grid = 1184;
-    if (grid < 1) grid = 1;
-    k_absmax<<<grid, RT, 0, st>>>(v, n, out);
+int launch_rhs_absmax(const double* v, int n, int ld, int nrhs, unsigned long long* out, cudaStream_t st) {
+    LP_CUDA(cudaMemsetAsync(out, 0, sizeof(unsigned long long) * nrhs, st));
+    int gx = (n + RT - 1) / RT;
+    if (gx > 64) gx = 64;
+    if (gx < 1) gx = 1;
+    k_rhs_absmax<<<dim3(gx, nrhs), RT, 0, st>>>(v, n, ld, out);
     count_launch();
     LP_CUDA(cudaGetLastError());
     return LP_OK;

@@ -208,7 +208,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     }
     int herr = 0;
     LP_CUDA(cudaMemcpyAsync(&herr, c->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
-    LP_CUDA(cudaStreamSynchronize(st));
+    LP_CHECK(wait_stream(c, st));
     if (herr != 0)
         return fail(LP_E_TIMEOUT, "tensor-core trailing update: a bounded wait expired (code " +
                                       std::to_string(herr) + "); the update was abandoned");

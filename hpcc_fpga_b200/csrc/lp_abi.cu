@@ -49,6 +49,12 @@ void Workspace::release() {
     cap = 0;
 }
 
+int wait_stream(lp_ctx* c, cudaStream_t st) {
+    LP_CUDA(cudaEventRecord(c->ev_block, st));
+    LP_CUDA(cudaEventSynchronize(c->ev_block));
+    return LP_OK;
+}
+
 int validate_matrix(const void* a, int n, int lda, int bs, const char* who) {
     if (a == nullptr) return fail(LP_E_INVALID, std::string(who) + ": null matrix pointer");
     if (n <= 0) return fail(LP_E_INVALID, std::string(who) + ": n must be positive");
@@ -325,6 +331,7 @@ int lp_ctx_create(int device, lp_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->aux, cudaStreamNonBlocking, prio_hi);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_block, cudaEventDisableTiming | cudaEventBlockingSync);
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         lp_ctx_destroy(c);
@@ -344,6 +351,7 @@ int lp_ctx_destroy(lp_ctx* c) {
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
     if (c->ev_fork != nullptr) cudaEventDestroy(c->ev_fork);
     if (c->ev_join != nullptr) cudaEventDestroy(c->ev_join);
+    if (c->ev_block != nullptr) cudaEventDestroy(c->ev_block);
     if (c->aux != nullptr) cudaStreamDestroy(c->aux);
     if (c->stream != nullptr) cudaStreamDestroy(c->stream);
     delete c;

@@ -67,7 +67,8 @@ int gesl_inv_init_attrs();
 int launch_residual_f64(const float* a, int lda, int n, const double* x, int ldx, const double* b, int ldb,
                         double* r, int ldr, int nrhs, cudaStream_t s);
 int launch_colabs(const float* a, int lda, int n, double* out, cudaStream_t s);
-int launch_absmax(const double* v, size_t n, unsigned long long* out, cudaStream_t s);
+// out[q] = max_i |v[q*ld + i]| (as the bits of a non-negative double), +inf if any is not finite.
+int launch_rhs_absmax(const double* v, int n, int ld, int nrhs, unsigned long long* out, cudaStream_t s);
 int launch_axpy_f64(double* x, const float* d, size_t n, cudaStream_t s);
 int launch_f64_to_f32(float* y, const double* v, size_t n, cudaStream_t s);
 int launch_f32_to_f64(double* y, const float* v, size_t n, cudaStream_t s);

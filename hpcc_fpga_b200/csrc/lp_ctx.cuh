@@ -46,6 +46,8 @@ constexpr int kBatchSolveOnly = 1 << 8;
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
                 int max_iters, int* iters, double* resid, cudaStream_t st);
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
+// Waits for the work queued on st so far without spinning a CPU core.
+int wait_stream(lp_ctx* c, cudaStream_t st);
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                     double* x, int max_iters, lp_timing* t);
 
@@ -63,6 +65,7 @@ struct lp_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t aux = nullptr;               // second (high-priority) stream for concurrent panel work
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_block = nullptr;           // blocking-sync event: waits yield the CPU instead of spinning
     cudaEvent_t ev[8] = {nullptr};
     lp::Workspace lt;    // transposed left panels (2 x bs x n, alternating by block step)
     lp::Workspace dsub;  // transposed diagonal sub-blocks of the blocked top stage (per stream)
@@ -74,6 +77,9 @@ struct lp_ctx {
     lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
+    lp::Workspace dnorm;                      // refinement norms (device)
+    unsigned long long* hnorm = nullptr;      // their pinned host copy
+    size_t hnorm_cap = 0;
     lp::Workspace bsys, bnext;                // batched: sorted system descriptors, work counter
     lp::Workspace tA, tB;                     // batched autotuner: scratch copies of the inputs
     uint64_t bsys_hash = 0;                   // descriptors + configuration of the cached graph
@@ -88,11 +94,14 @@ struct lp_ctx {
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
         lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
-                                &bsys, &bnext, &tA, &tB};
+                                &dnorm, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
         bgraph = nullptr;
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();
+        if (hnorm != nullptr) cudaFreeHost(hnorm);
+        hnorm = nullptr;
+        hnorm_cap = 0;
     }
 };

@@ -32,6 +32,7 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <list>
 #include <mutex>
 #include <thread>
 #include <unordered_map>
@@ -69,6 +70,20 @@ __global__ void k_pad_identity(float* a, int ld, int n, int npad) {
             c = n + k % p;
         }
         a[r * ld + c] = (r == c) ? 1.0f : 0.0f;
+    }
+}
+
+// Copies of float4 runs, one CTA per run: the wave's new originals into the
+// factor buffers that the batched kernel factors in place.
+struct CopyRun {
+    const float4* src;
+    float4* dst;
+    long long n4;
+};
+__global__ void k_copy_runs(const CopyRun* __restrict__ runs, int count) {
+    for (int t = blockIdx.x; t < count; t += gridDim.x) {
+        const CopyRun r = runs[t];
+        for (long long i = threadIdx.x; i < r.n4; i += blockDim.x) r.dst[i] = r.src[i];
     }
 }
 
@@ -179,6 +194,8 @@ struct Entry {
     int users = 0;       // in-flight requests holding it
     bool ready = false;  // factors written
     bool cached = true;  // in the key map (false: private to one request)
+    bool in_lru = false;
+    std::list<Entry*>::iterator lru_pos;
 };
 
 struct Req {
@@ -189,7 +206,10 @@ struct Req {
     size_t reserve = 0;  // per-request vectors charged to the budget
 };
 
-int pad_block(int n) { return n <= 2048 ? 128 : 256; }
+// Factorization block of the slot path: 128 is the fastest for every n the
+// server accepts, in FP32 and in the tensor-core precisions (measured on B200
+// against 256 and 512 for n = 1024 .. 8192).
+int pad_block(int) { return 128; }
 int round4(int n) { return (n + 3) / 4 * 4; }
 // FP32 / FP64 right-hand-side, solution and residual vectors of one request
 size_t vec_bytes(int n, int nrhs) { return (size_t)nrhs * (size_t)(n + 256) * 40 + (size_t)(n + 256) * 8; }
@@ -207,7 +227,12 @@ using namespace lp;
 struct lp_worker {
     lp_ctx* c = nullptr;
     bool wave = false;
-    Workspace sys, items, next, resid, b0, x32, x64, b32;
+    bool large_only = false;       // slot reserved for systems with n > large_n
+    cudaStream_t base = nullptr;   // the context's own main stream
+    cudaStream_t high = nullptr;   // main stream for systems with n > large_n (higher priority)
+    Workspace sys, items, next, resid, b0, x32, x64, b32, runs;
+    char* stage = nullptr;         // pinned host staging of a wave's descriptors and residuals
+    size_t stage_cap = 0;          // systems it holds
 };
 
 struct lp_server {
@@ -218,15 +243,19 @@ struct lp_server {
     std::vector<lp_worker*> workers;
     std::vector<std::thread> threads;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_ready;
+    int ready = 0;                 // workers through their warm-up
+    int start_status = LP_OK;
     std::deque<Req*> pending;
     std::deque<lp_result> done;
     std::unordered_map<long long, Entry*> cache;
+    std::list<Entry*> lru;  // ready cached entries, least recently used first
     size_t used = 0;
     long long next_id = 1;
     bool stop = false;
     int running = 0;
     long long completed = 0, waves = 0, waved_systems = 0, evictions = 0, rejected = 0;
+    double slot_busy = 0.0, wave_busy = 0.0;
 };
 
 namespace lp {
@@ -242,6 +271,7 @@ void release_slab(lp_server* s, Slab* sl) {
 }
 
 void drop_entry(lp_server* s, Entry* e) {
+    if (e->in_lru) s->lru.erase(e->lru_pos);
     if (e->cached) {
         auto it = s->cache.find(e->key);
         if (it != s->cache.end() && it->second == e) s->cache.erase(it);
@@ -254,10 +284,11 @@ bool make_room(lp_server* s, size_t need) {
     const size_t budget = (size_t)s->cfg.hbm_budget_bytes;
     while (s->used + need > budget) {
         Entry* victim = nullptr;
-        for (auto& kv : s->cache) {
-            Entry* e = kv.second;
-            if (e->ready && e->users == 0 && (victim == nullptr || e->last_used < victim->last_used)) victim = e;
-        }
+        for (Entry* e : s->lru)  // in-flight entries are few: the first idle one is close to the front
+            if (e->users == 0) {
+                victim = e;
+                break;
+            }
         if (victim == nullptr) return false;
         drop_entry(s, victim);
         s->evictions++;
@@ -275,7 +306,15 @@ void finish_locked(lp_server* s, Req* r, int status) {
         e->last_used = r->res.t_done;
         if (status == LP_OK) {
             e->ready = true;
-            if (!e->cached && e->users == 0) drop_entry(s, e);
+            if (e->cached) {  // most recently used at the back
+                if (e->in_lru)
+                    s->lru.splice(s->lru.end(), s->lru, e->lru_pos);
+                else
+                    e->lru_pos = s->lru.insert(s->lru.end(), e);
+                e->in_lru = true;
+            } else if (e->users == 0) {
+                drop_entry(s, e);
+            }
         } else if (!e->ready && e->users == 0) {
             drop_entry(s, e);  // its factors were never completed
         }
@@ -347,7 +386,20 @@ int admit(lp_server* s, Req* r, bool wave) {
 
 // ---- slot path: one system through the blocked factorization ----
 
+int run_slot_on(lp_server* s, lp_worker* w, Req* r);
+
+// Systems above large_n define the latency tail: their bulk work runs on the
+// worker's higher-priority stream (the panels are on the top-priority
+// auxiliary stream either way).
 int run_slot(lp_server* s, lp_worker* w, Req* r) {
+    const bool large = r->q.n > s->cfg.large_n && w->high != nullptr;
+    if (large) w->c->stream = w->high;
+    const int st = run_slot_on(s, w, r);
+    w->c->stream = w->base;
+    return st;
+}
+
+int run_slot_on(lp_server* s, lp_worker* w, Req* r) {
     lp_ctx* c = w->c;
     cudaStream_t st = c->stream;
     const lp_request& q = r->q;
@@ -391,7 +443,7 @@ int run_slot(lp_server* s, lp_worker* w, Req* r) {
     if (rs != LP_OK && rs != LP_E_NUMERIC) return rs;
     LP_CUDA(cudaMemcpy2DAsync(q.X, sizeof(double) * q.ldx, x, sizeof(double) * n, sizeof(double) * n, nrhs,
                               cudaMemcpyDeviceToHost, st));
-    LP_CUDA(cudaStreamSynchronize(st));
+    LP_CHECK(wait_stream(c, st));
     // refine_core normalizes with DBL_EPSILON/2; the FP32 mode states its own unit roundoff
     r->res.hpl_resid = prec == LP_F32 ? resid * (DBL_EPSILON / FLT_EPSILON) : resid;
     r->res.ir_iters = iters;
@@ -400,44 +452,44 @@ int run_slot(lp_server* s, lp_worker* w, Req* r) {
 
 // ---- wave path: many systems in one batched launch ----
 
+// Pinned staging per system: lp_system + WaveItem + CopyRun + one residual.
+constexpr size_t kStagePer = sizeof(lp_system) + sizeof(WaveItem) + sizeof(CopyRun) + sizeof(double);
+
+int ensure_stage(lp_worker* w, size_t count) {
+    if (w->stage_cap >= count) return LP_OK;
+    if (w->stage != nullptr) cudaFreeHost(w->stage);
+    w->stage = nullptr;
+    w->stage_cap = 0;
+    LP_CUDA(cudaMallocHost(&w->stage, kStagePer * count));
+    w->stage_cap = count;
+    return LP_OK;
+}
+
 int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
     lp_ctx* c = w->c;
     cudaStream_t st = c->stream;
     const int prec = s->cfg.precision;
     std::stable_sort(rs.begin(), rs.end(), [](const Req* a, const Req* b) { return a->q.n > b->q.n; });
     const int count = (int)rs.size();
-    // one slab for the wave's new systems: factors [0, tot), originals [tot, 2 tot)
-    size_t tot = 0, vtot = 0;
-    std::vector<size_t> aoff(count), voff(count);
+    // vectors of all systems; a slab (factors, then the original) per new system
+    size_t vtot = 0;
+    std::vector<size_t> voff(count);
     for (int i = 0; i < count; i++) {
-        const int n = rs[i]->q.n, ld = round4(n);
-        aoff[i] = tot;
-        if (!rs[i]->hit) tot += (size_t)n * ld;
         voff[i] = vtot;
-        vtot += (size_t)rs[i]->q.nrhs * ld;
+        vtot += (size_t)rs[i]->q.nrhs * round4(rs[i]->q.n);
     }
-    float* fbase = nullptr;
-    if (tot > 0) {
-        void* p = nullptr;
-        LP_CUDA(cudaMallocFromPoolAsync(&p, 2 * sizeof(float) * tot, s->pool, st));
-        fbase = static_cast<float*>(p);
-        std::lock_guard<std::mutex> lock(s->mu);
-        Slab* slab = new Slab();
-        slab->ptr = p;
-        for (Req* r : rs)
-            if (!r->hit) {  // merge the charged placeholders into the shared slab
-                slab->bytes += r->entry->slab->bytes;
-                slab->refs++;
-                delete r->entry->slab;
-                r->entry->slab = slab;
-            }
-    }
-    for (int i = 0; i < count; i++)
-        if (!rs[i]->hit) {
-            Entry* e = rs[i]->entry;
+    std::vector<CopyRun> dup;
+    for (Req* r : rs)
+        if (!r->hit) {
+            Entry* e = r->entry;
+            void* p = nullptr;
+            LP_CUDA(cudaMallocFromPoolAsync(&p, e->slab->bytes, s->pool, st));
+            e->slab->ptr = p;
             e->ld = round4(e->n);
-            e->lu = fbase + aoff[i];
-            e->a0 = fbase + tot + aoff[i];
+            e->lu = static_cast<float*>(p);
+            e->a0 = e->lu + (size_t)e->n * e->ld;
+            dup.push_back(CopyRun{reinterpret_cast<const float4*>(e->a0), reinterpret_cast<float4*>(e->lu),
+                                  (long long)e->n * e->ld / 4});
         }
     LP_CHECK(w->b0.ensure(sizeof(float) * vtot));
     LP_CHECK(w->x32.ensure(sizeof(float) * vtot));
@@ -458,7 +510,21 @@ int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
         LP_CUDA(cudaMemcpy2DAsync(b0 + voff[i], sizeof(float) * round4(q.n), q.B, sizeof(float) * q.ldb,
                                   sizeof(float) * q.n, q.nrhs, cudaMemcpyHostToDevice, st));
     }
-    if (tot > 0) LP_CUDA(cudaMemcpyAsync(fbase, fbase + tot, sizeof(float) * tot, cudaMemcpyDeviceToDevice, st));
+    LP_CHECK(ensure_stage(w, (size_t)count));
+    lp_system* h_sys = reinterpret_cast<lp_system*>(w->stage);
+    WaveItem* h_items = reinterpret_cast<WaveItem*>(w->stage + sizeof(lp_system) * w->stage_cap);
+    CopyRun* h_runs = reinterpret_cast<CopyRun*>(w->stage + (sizeof(lp_system) + sizeof(WaveItem)) * w->stage_cap);
+    double* h_res =
+        reinterpret_cast<double*>(w->stage + (sizeof(lp_system) + sizeof(WaveItem) + sizeof(CopyRun)) * w->stage_cap);
+    if (!dup.empty()) {
+        LP_CHECK(w->runs.ensure(sizeof(CopyRun) * dup.size()));
+        std::memcpy(h_runs, dup.data(), sizeof(CopyRun) * dup.size());
+        LP_CUDA(cudaMemcpyAsync(w->runs.ptr, h_runs, sizeof(CopyRun) * dup.size(), cudaMemcpyHostToDevice, st));
+        k_copy_runs<<<std::min((int)dup.size(), 4 * c->num_sms), 256, 0, st>>>(static_cast<CopyRun*>(w->runs.ptr),
+                                                                                (int)dup.size());
+        count_launch();
+        LP_CUDA(cudaGetLastError());
+    }
     LP_CUDA(cudaMemcpyAsync(x32, b0, sizeof(float) * vtot, cudaMemcpyDeviceToDevice, st));
 
     std::vector<lp_system> sys(count);
@@ -474,24 +540,25 @@ int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
     lp_batch_config bc;
     lp_batch_default_config(&bc);
     const double eps = prec == LP_F32 ? FLT_EPSILON / 2.0 : DBL_EPSILON / 2.0;
-    std::vector<double> res(count);
     // batched kernel on the first m descriptors, then the residual of those systems
     auto step = [&](const std::vector<lp_system>& d, const std::vector<WaveItem>& wi) -> int {
         const int m = (int)d.size();
-        LP_CUDA(cudaMemcpyAsync(w->sys.ptr, d.data(), sizeof(lp_system) * m, cudaMemcpyHostToDevice, st));
-        LP_CUDA(cudaMemcpyAsync(w->items.ptr, wi.data(), sizeof(WaveItem) * m, cudaMemcpyHostToDevice, st));
+        std::memcpy(h_sys, d.data(), sizeof(lp_system) * m);
+        std::memcpy(h_items, wi.data(), sizeof(WaveItem) * m);
+        LP_CUDA(cudaMemcpyAsync(w->sys.ptr, h_sys, sizeof(lp_system) * m, cudaMemcpyHostToDevice, st));
+        LP_CUDA(cudaMemcpyAsync(w->items.ptr, h_items, sizeof(WaveItem) * m, cudaMemcpyHostToDevice, st));
         LP_CHECK(launch_batch(c, static_cast<lp_system*>(w->sys.ptr), m, nullptr, nullptr, bc,
                               static_cast<int*>(w->next.ptr), st, true));
         k_wave_residual<<<std::min(m, 4 * c->num_sms), kRT, 0, st>>>(static_cast<WaveItem*>(w->items.ptr), m, eps,
                                                                       static_cast<double*>(w->resid.ptr));
         count_launch();
         LP_CUDA(cudaGetLastError());
-        LP_CUDA(cudaMemcpyAsync(res.data(), w->resid.ptr, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
-        LP_CUDA(cudaStreamSynchronize(st));
+        LP_CUDA(cudaMemcpyAsync(h_res, w->resid.ptr, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+        LP_CHECK(wait_stream(c, st));
         return LP_OK;
     };
     LP_CHECK(step(sys, items));
-    std::vector<double> final_res(res.begin(), res.end());
+    std::vector<double> final_res(h_res, h_res + count);
     std::vector<int> iters(count, 0);
     if (prec != LP_F32) {
         // batched refinement of the systems above the bound: d = LU \ r (solve only), x += d
@@ -512,7 +579,7 @@ int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
             }
             LP_CHECK(step(d, wi));
             for (size_t k = 0; k < idx.size(); k++) {
-                final_res[idx[k]] = res[k];
+                final_res[idx[k]] = h_res[k];
                 iters[idx[k]]++;
             }
         }
@@ -522,7 +589,7 @@ int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
         LP_CUDA(cudaMemcpy2DAsync(q.X, sizeof(double) * q.ldx, x64 + voff[i], sizeof(double) * round4(q.n),
                                   sizeof(double) * q.n, q.nrhs, cudaMemcpyDeviceToHost, st));
     }
-    LP_CUDA(cudaStreamSynchronize(st));
+    LP_CHECK(wait_stream(c, st));
     for (int i = 0; i < count; i++) {
         rs[i]->res.hpl_resid = final_res[i];
         rs[i]->res.ir_iters = iters[i];
@@ -530,11 +597,74 @@ int run_wave(lp_server* s, lp_worker* w, std::vector<Req*>& rs) {
     return LP_OK;
 }
 
+// ---- warm-up (lp_server_config::warm_n) ----
+
+// Factor and solve an identity of order warm_n with the maximum number of
+// right-hand sides on the slot's stream, so every workspace of the slot path
+// reaches its final size before the first request.
+int warm_slot(lp_server* s, lp_worker* w) {
+    lp_ctx* c = w->c;
+    cudaStream_t st = c->stream;
+    const int bs = pad_block(s->cfg.warm_n), npad = (s->cfg.warm_n + bs - 1) / bs * bs;
+    const size_t nn = (size_t)npad * npad, nv = (size_t)npad * kMaxRhs;
+    void* p = nullptr;
+    LP_CUDA(cudaMallocFromPoolAsync(&p, 2 * sizeof(float) * nn, s->pool, st));
+    float* lu = static_cast<float*>(p);
+    float* a0 = lu + nn;
+    int rc = LP_OK;
+    auto run = [&]() -> int {
+        k_pad_identity<<<2 * c->num_sms, 256, 0, st>>>(a0, npad, 0, npad);
+        count_launch();
+        LP_CUDA(cudaGetLastError());
+        LP_CUDA(cudaMemcpyAsync(lu, a0, sizeof(float) * nn, cudaMemcpyDeviceToDevice, st));
+        if (s->cfg.precision == LP_F32)
+            LP_CHECK(gefa_f32(c, lu, npad, npad, bs, st));
+        else
+            LP_CHECK(gefa_mixed(c, s->cfg.precision, lu, npad, npad, bs, st));
+        LP_CHECK(w->b32.ensure(sizeof(float) * nv));
+        LP_CHECK(c->dB64.ensure(sizeof(double) * nv));
+        LP_CHECK(c->dX.ensure(sizeof(double) * nv));
+        // right-hand sides: the first rows of the identity
+        LP_CUDA(cudaMemcpyAsync(w->b32.ptr, a0, sizeof(float) * nv, cudaMemcpyDeviceToDevice, st));
+        LP_CHECK(launch_f32_to_f64(static_cast<double*>(c->dB64.ptr), static_cast<float*>(w->b32.ptr), nv, st));
+        int iters = 0;
+        double resid = 0.0;
+        return refine_core(c, a0, npad, lu, npad, static_cast<double*>(c->dB64.ptr),
+                           static_cast<double*>(c->dX.ptr), kMaxRhs, 1, &iters, &resid, st);
+    };
+    rc = run();
+    cudaFreeAsync(p, st);
+    const int ws = wait_stream(c, st);
+    return rc != LP_OK ? rc : ws;
+}
+
+// Size a wave worker's scratch for the largest wave the configuration allows.
+int warm_wave(lp_server* s, lp_worker* w) {
+    const size_t count = (size_t)s->cfg.batch_max_count;
+    const size_t vtot = count * kMaxRhs * (size_t)round4(s->cfg.batch_max_n);
+    LP_CHECK(w->b0.ensure(sizeof(float) * vtot));
+    LP_CHECK(w->x32.ensure(sizeof(float) * vtot));
+    LP_CHECK(w->x64.ensure(sizeof(double) * vtot));
+    LP_CHECK(w->sys.ensure(sizeof(lp_system) * count));
+    LP_CHECK(w->items.ensure(sizeof(WaveItem) * count));
+    LP_CHECK(w->resid.ensure(sizeof(double) * count));
+    LP_CHECK(w->next.ensure(sizeof(int)));
+    LP_CHECK(w->runs.ensure(sizeof(CopyRun) * count));
+    return ensure_stage(w, count);
+}
+
 // ---- worker threads ----
 
 void worker_loop(lp_server* s, lp_worker* w) {
     cudaSetDevice(s->device);
     const bool per_request = s->cfg.mode == LP_SERVE_PER_REQUEST;
+    {
+        const int st = s->cfg.warm_n > 0 ? (w->wave ? warm_wave(s, w) : warm_slot(s, w)) : LP_OK;
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (st != LP_OK && s->start_status == LP_OK) s->start_status = st;
+        s->ready++;
+        s->cv_ready.notify_all();
+    }
     for (;;) {
         std::vector<Req*> take;
         {
@@ -544,7 +674,7 @@ void worker_loop(lp_server* s, lp_worker* w) {
                 for (auto it = s->pending.begin(); it != s->pending.end();) {
                     Req* r = *it;
                     const bool small = !per_request && r->q.n <= s->cfg.batch_max_n;
-                    if (small != w->wave) {
+                    if (small != w->wave || (w->large_only && r->q.n <= s->cfg.large_n)) {
                         ++it;
                         continue;
                     }
@@ -565,9 +695,11 @@ void worker_loop(lp_server* s, lp_worker* w) {
                 s->cv_work.wait(lock);
             }
         }
+        const double t0 = now_s();
         const int st = w->wave ? run_wave(s, w, take) : run_slot(s, w, take[0]);
         {
             std::lock_guard<std::mutex> lock(s->mu);
+            (w->wave ? s->wave_busy : s->slot_busy) += now_s() - t0;
             if (w->wave) {
                 s->waves++;
                 s->waved_systems += (long long)take.size();
@@ -602,11 +734,15 @@ int lp_server_default_config(lp_server_config* cfg) {
     cfg->hbm_budget_bytes = 80ll * 1000 * 1000 * 1000;
     cfg->mode = LP_SERVE_CONTINUOUS;
     cfg->precision = LP_F32;
-    cfg->slots = 4;
+    cfg->slots = 6;
     cfg->batch_workers = 2;
-    cfg->batch_max_n = 1024;
+    cfg->batch_max_n = 512;
     cfg->batch_max_count = 1024;
     cfg->max_refinements = 50;
+    cfg->warm_n = 0;
+    cfg->reserve_bytes = 0;
+    cfg->large_n = 2048;
+    cfg->large_slots = 2;
     return LP_OK;
 }
 
@@ -621,7 +757,9 @@ int lp_server_start(int device, const lp_server_config* cfg, lp_server** out) {
     if (c.hbm_budget_bytes <= 0 || (c.mode != LP_SERVE_CONTINUOUS && c.mode != LP_SERVE_PER_REQUEST) ||
         (c.precision != LP_F32 && c.precision != LP_BF16_IR && c.precision != LP_FP8_IR) || c.slots < 1 ||
         c.slots > 16 || c.batch_workers < 1 || c.batch_workers > 4 || c.batch_max_n < 0 ||
-        c.batch_max_n > kWaveMaxN || c.batch_max_count < 1 || c.max_refinements < 0)
+        c.batch_max_n > kWaveMaxN || c.batch_max_count < 1 || c.max_refinements < 0 || c.warm_n < 0 ||
+        c.warm_n > kMaxN || c.reserve_bytes < 0 || c.large_n < 0 ||
+        c.large_slots < 0)
         return fail(LP_E_INVALID, "lp_server_start: bad configuration");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -636,6 +774,7 @@ int lp_server_start(int device, const lp_server_config* cfg, lp_server** out) {
     auto undo = [&](int st) {
         for (auto* w : s->workers) {
             if (w->c) lp_ctx_destroy(w->c);
+            if (w->high) cudaStreamDestroy(w->high);
             delete w;
         }
         if (s->free_stream) cudaStreamDestroy(s->free_stream);
@@ -655,17 +794,43 @@ int lp_server_start(int device, const lp_server_config* cfg, lp_server** out) {
     if (e != cudaSuccess) return undo(cuda_fail(e, "cudaMemPoolSetAttribute", __FILE__, __LINE__));
     e = cudaStreamCreateWithFlags(&s->free_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return undo(cuda_fail(e, "cudaStreamCreate", __FILE__, __LINE__));
+    if (c.reserve_bytes > 0) {  // map the memory now; the release threshold keeps it in the pool
+        void* p = nullptr;
+        e = cudaMallocFromPoolAsync(&p, (size_t)c.reserve_bytes, s->pool, s->free_stream);
+        if (e == cudaSuccess) e = cudaFreeAsync(p, s->free_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->free_stream);
+        if (e != cudaSuccess) return undo(cuda_fail(e, "lp_server_start: pool reservation", __FILE__, __LINE__));
+    }
     const bool per_request = c.mode == LP_SERVE_PER_REQUEST;
     const int nslots = per_request ? 1 : c.slots;
     const int nwaves = per_request || c.batch_max_n == 0 ? 0 : c.batch_workers;
+    int prio_least = 0, prio_greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    const int prio_large = prio_greatest < prio_least ? prio_greatest + 1 : prio_least;
     for (int i = 0; i < nslots + nwaves; i++) {
         lp_worker* w = new lp_worker();
         w->wave = i >= nslots;
+        w->large_only = !per_request && i < std::min(c.large_slots, c.slots - 1);
         s->workers.push_back(w);
         const int st = lp_ctx_create(device, &w->c);
         if (st != LP_OK) return undo(st);
+        w->base = w->c->stream;
+        if (!w->wave && !per_request) {
+            e = cudaStreamCreateWithPriority(&w->high, cudaStreamNonBlocking, prio_large);
+            if (e != cudaSuccess) return undo(cuda_fail(e, "cudaStreamCreateWithPriority", __FILE__, __LINE__));
+        }
     }
     for (auto* w : s->workers) s->threads.emplace_back(worker_loop, s, w);
+    int st = LP_OK;
+    {
+        std::unique_lock<std::mutex> lock(s->mu);
+        s->cv_ready.wait(lock, [&] { return s->ready == (int)s->workers.size(); });
+        st = s->start_status;
+    }
+    if (st != LP_OK) {
+        lp_server_stop(s);
+        return fail(st, "lp_server_start: worker warm-up failed");
+    }
     *out = s;
     return LP_OK;
 }
@@ -686,9 +851,11 @@ int lp_server_stop(lp_server* s) {
     for (Entry* e : all) drop_entry(s, e);
     cudaStreamSynchronize(s->free_stream);
     for (auto* w : s->workers) {
-        Workspace* ws[] = {&w->sys, &w->items, &w->next, &w->resid, &w->b0, &w->x32, &w->x64, &w->b32};
+        Workspace* ws[] = {&w->sys, &w->items, &w->next, &w->resid, &w->b0, &w->x32, &w->x64, &w->b32, &w->runs};
         for (auto* x : ws) x->release();
         lp_ctx_destroy(w->c);
+        if (w->high) cudaStreamDestroy(w->high);
+        if (w->stage) cudaFreeHost(w->stage);
         delete w;
     }
     cudaStreamDestroy(s->free_stream);
@@ -753,6 +920,11 @@ int lp_server_get_info(lp_server* s, lp_server_info* info) {
     info->waved_systems = s->waved_systems;
     info->evictions = s->evictions;
     info->rejected = s->rejected;
+    uint64_t reserved = 0;
+    cudaMemPoolGetAttribute(s->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    info->pool_reserved_bytes = (long long)reserved;
+    info->slot_busy_s = s->slot_busy;
+    info->wave_busy_s = s->wave_busy;
     return LP_OK;
 }
 

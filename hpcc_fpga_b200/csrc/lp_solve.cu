@@ -7,6 +7,7 @@
 // with the factorization and the host copies.
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "lp_ctx.cuh"
@@ -19,58 +20,63 @@ static float ev_s(cudaEvent_t a, cudaEvent_t b) {
     return ms * 1e-3f;
 }
 
+// Bits of a non-negative double written by launch_rhs_absmax.
+static double from_bits(unsigned long long b) {
+    double d;
+    std::memcpy(&d, &b, sizeof(d));
+    return d;
+}
+
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
                 int max_iters, int* iters_out, double* resid_out, cudaStream_t st) {
     const size_t nv = (size_t)n * nrhs;
     LP_CHECK(c->dB.ensure(sizeof(float) * nv));
     LP_CHECK(c->dR.ensure(sizeof(double) * nv));
     LP_CHECK(c->dCol.ensure(sizeof(double) * (size_t)n));
+    // norm slots: [0] ||M||, [1] unused, [2, 2+q) ||b_q||, then ||r_q||, then ||x_q||
+    const size_t slots = 2 + 3 * (size_t)nrhs;
+    LP_CHECK(c->dnorm.ensure(sizeof(unsigned long long) * slots));
+    if (c->hnorm_cap < slots) {
+        if (c->hnorm != nullptr) cudaFreeHost(c->hnorm);
+        c->hnorm = nullptr;
+        c->hnorm_cap = 0;
+        const size_t cap = slots < 64 ? 64 : slots;  // up to 20 right-hand sides without regrowth
+        LP_CUDA(cudaMallocHost(&c->hnorm, sizeof(unsigned long long) * cap));
+        c->hnorm_cap = cap;
+    }
     float* dB = static_cast<float*>(c->dB.ptr);
     double* dR = static_cast<double*>(c->dR.ptr);
     double* dCol = static_cast<double*>(c->dCol.ptr);
+    unsigned long long* dn = static_cast<unsigned long long*>(c->dnorm.ptr);
+    unsigned long long* rn = dn + 2 + nrhs;
+    unsigned long long* xn = rn + nrhs;
 
     LP_CHECK(launch_colabs(a0, lda, n, dCol, st));
+    LP_CHECK(launch_rhs_absmax(dCol, n, n, 1, dn, st));
+    LP_CHECK(launch_rhs_absmax(b64, n, n, nrhs, dn + 2, st));
     LP_CHECK(launch_f64_to_f32(dB, b64, nv, st));
     LP_CHECK(gesl_f32(c, lu, n, lda, dB, nrhs, n, st));
     LP_CHECK(launch_f32_to_f64(x, dB, nv, st));
     LP_CUDA(cudaEventRecord(c->ev[4], st));  // end of the first solve
-
-    std::vector<double> col(n), hx(nv), hr(nv), hb(nv);
-    LP_CUDA(cudaMemcpyAsync(col.data(), dCol, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
-    LP_CUDA(cudaMemcpyAsync(hb.data(), b64, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
-    double normA = -1.0;
-    std::vector<double> normb(nrhs, 0.0);
 
     const double eps = DBL_EPSILON / 2.0;
     double resid = INFINITY;
     int iters = 0;
     auto measure = [&]() -> int {
         LP_CHECK(launch_residual_f64(a0, lda, n, x, n, b64, n, dR, n, nrhs, st));
-        LP_CUDA(cudaMemcpyAsync(hx.data(), x, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
-        LP_CUDA(cudaMemcpyAsync(hr.data(), dR, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
-        LP_CUDA(cudaStreamSynchronize(st));
-        if (normA < 0.0) {
-            normA = 0.0;
-            for (int i = 0; i < n; i++) normA = std::fmax(normA, col[i]);
-            for (int q = 0; q < nrhs; q++)
-                for (int i = 0; i < n; i++) normb[q] = std::fmax(normb[q], std::fabs(hb[(size_t)q * n + i]));
-        }
+        LP_CHECK(launch_rhs_absmax(dR, n, n, nrhs, rn, st));
+        LP_CHECK(launch_rhs_absmax(x, n, n, nrhs, xn, st));
+        LP_CUDA(cudaMemcpyAsync(c->hnorm, dn, sizeof(unsigned long long) * slots, cudaMemcpyDeviceToHost, st));
+        LP_CHECK(wait_stream(c, st));
+        const unsigned long long* h = c->hnorm;
+        const double normA = from_bits(h[0]);
         resid = 0.0;
-        bool finite = true;
+        bool finite = std::isfinite(normA);
         for (int q = 0; q < nrhs && finite; q++) {
-            double rn = 0.0, xn = 0.0;
-            for (int i = 0; i < n; i++) {
-                const double ri = hr[(size_t)q * n + i], xi = hx[(size_t)q * n + i];
-                if (!std::isfinite(ri) || !std::isfinite(xi)) {
-                    finite = false;  // fmax would silently drop a NaN
-                    break;
-                }
-                rn = std::fmax(rn, std::fabs(ri));
-                xn = std::fmax(xn, std::fabs(xi));
-            }
-            const double rq = rn / (normA * xn + normb[q]) / (double)n / eps;
-            if (!std::isfinite(rq)) finite = false;
-            resid = std::fmax(resid, rq);
+            const double rq = from_bits(h[2 + nrhs + q]), xq = from_bits(h[2 + 2 * nrhs + q]);
+            const double r = rq / (normA * xq + from_bits(h[2 + q])) / (double)n / eps;
+            if (!std::isfinite(rq) || !std::isfinite(xq) || !std::isfinite(r)) finite = false;  // fmax drops NaN
+            resid = std::fmax(resid, r);
         }
         if (!finite) resid = NAN;
         return LP_OK;

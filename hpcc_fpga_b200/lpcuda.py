@@ -86,7 +86,8 @@ LP_SERVE_CONTINUOUS, LP_SERVE_PER_REQUEST = 0, 1
 class LpServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("mode", ctypes.c_int), ("precision", ctypes.c_int),
                 ("slots", ctypes.c_int), ("batch_workers", ctypes.c_int), ("batch_max_n", ctypes.c_int),
-                ("batch_max_count", ctypes.c_int), ("max_refinements", ctypes.c_int)]
+                ("batch_max_count", ctypes.c_int), ("max_refinements", ctypes.c_int), ("warm_n", ctypes.c_int),
+                ("reserve_bytes", ctypes.c_longlong), ("large_n", ctypes.c_int), ("large_slots", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {f[0]: getattr(self, f[0]) for f in self._fields_}
@@ -111,7 +112,8 @@ class LpServerInfo(ctypes.Structure):
     _fields_ = [("pending", ctypes.c_int), ("running", ctypes.c_int), ("resident", ctypes.c_int),
                 ("used_bytes", ctypes.c_longlong), ("completed", ctypes.c_longlong), ("waves", ctypes.c_longlong),
                 ("waved_systems", ctypes.c_longlong), ("evictions", ctypes.c_longlong),
-                ("rejected", ctypes.c_longlong)]
+                ("rejected", ctypes.c_longlong), ("pool_reserved_bytes", ctypes.c_longlong),
+                ("slot_busy_s", ctypes.c_double), ("wave_busy_s", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {f[0]: getattr(self, f[0]) for f in self._fields_}

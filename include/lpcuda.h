@@ -272,6 +272,14 @@ typedef struct {
     int batch_max_n;            /* systems with n <= this (<= 1024) go to the batched kernel; 0: none */
     int batch_max_count;        /* systems per wave */
     int max_refinements;        /* FP64 refinement cap of the mixed precisions */
+    int warm_n;                 /* > 0: at start every slot factors and solves an order-warm_n system so its
+                                   workspaces are sized, and every wave worker sizes its scratch for the
+                                   largest wave; requests up to warm_n then allocate nothing outside the pool */
+    long long reserve_bytes;    /* > 0: at start the server's pool maps this much device memory and keeps it;
+                                   some headroom above the budget keeps fragmentation from growing the pool
+                                   (growing it stalls the device) */
+    int large_n;                /* systems with n > large_n run on higher-priority streams ... */
+    int large_slots;            /* ... and this many slots (at most slots - 1) take only them */
 } lp_server_config;
 typedef struct {
     long long key;              /* matrix identity: same key and n reuse resident factors */
@@ -302,6 +310,8 @@ typedef struct {
     int resident;               /* matrices with resident factors */
     long long used_bytes;       /* charged against the budget */
     long long completed, waves, waved_systems, evictions, rejected;
+    long long pool_reserved_bytes; /* device memory the server's pool holds (in use or kept for reuse) */
+    double slot_busy_s, wave_busy_s; /* summed worker time spent on requests, slot and wave workers */
 } lp_server_info;
 int lp_server_default_config(lp_server_config* cfg);
 /* Starts the worker threads, each with its own context.  cfg NULL: default. */

@@ -13,7 +13,8 @@ def test_default_config(lp):
     cfg = lp.server_config()
     assert cfg.hbm_budget_bytes == 80 * 10 ** 9
     assert cfg.mode == lp.LP_SERVE_CONTINUOUS and cfg.precision == lp.LP_F32
-    assert cfg.batch_max_n == 1024 and cfg.slots >= 1 and cfg.batch_workers >= 1
+    assert cfg.batch_max_n == 512 and cfg.slots == 6 and cfg.large_slots == 2 and cfg.batch_workers >= 1
+    assert cfg.warm_n == 0 and cfg.reserve_bytes == 0
     c2 = lp.server_config(precision="bf16", mode="per_request", slots=2)
     assert c2.precision == lp.LP_BF16_IR and c2.mode == lp.LP_SERVE_PER_REQUEST and c2.slots == 2
 
