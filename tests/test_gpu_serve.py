@@ -75,7 +75,7 @@ def test_alone_equals_mix_f32(lp, wl):
     for spec, r, x, (ra, xa) in zip(specs, mix, mix_x, alone):
         assert r["status"] == 0 and ra["status"] == 0
         assert np.array_equal(x, xa), f"request {spec} differs alone vs in the mix"
-        assert r["batched"] == (spec[1] <= 1024)
+        assert r["batched"] == (spec[1] <= lp.server_config().batch_max_n)
     _check_against_oracle(wl, specs, mix, mix_x, FLT_EPS)
     # the work overlapped: some requests ran at the same time
     iv = sorted((r["t_start"], r["t_done"]) for r in mix)
