@@ -4,13 +4,21 @@
 //
 // Aq: the left panel rounded to BF16 (or FP8 E4M3), m x k, k contiguous;
 // Bq: the top panel rounded the same way and stored transposed, n x k.
-// Both are K-major operands, loaded by TMA with 128-byte swizzle into a
-// STAGES-deep shared-memory ring; one elected thread issues tcgen05.mma
-// (kind::f16 for BF16, kind::f8f6f4 for E4M3) into a 128 x 128 FP32
-// accumulator in tensor memory; after the k loop the four warps read the
-// accumulator back with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile
-// rows) and add it into C, which is read and written once.  The diagonal
-// block and the triangular stages stay FP32 (k_lu.cu, k_trsm.cu).
+// Both are K-major operands.  Persistent, warp-specialized: one CTA per SM
+// walks 128 x 128 C tiles (row-block-major, so neighbouring CTAs share the A
+// tile in L2).
+//   warp 0      TMA producer: A and B tiles (128-byte swizzle) into a
+//               STAGES-deep shared-memory ring;
+//   warp 1      one elected thread issues tcgen05.mma (kind::f16 for BF16,
+//               kind::f8f6f4 for E4M3) into one of TWO 128-column FP32
+//               accumulators in tensor memory, alternating by tile;
+//   warps 2-9   epilogue: while the next tile's MMAs run, read the finished
+//               accumulator with tcgen05.ld (warp w reads TMEM lanes
+//               32*(w%4).., half (w-2)/4 of the columns), transpose each
+//               32 x 32 block through shared memory and add it into C with
+//               coalesced loads/stores (the C block is prefetched before the
+//               accumulator is ready).  C is read and written once.
+// The diagonal block and the triangular stages stay FP32 (k_lu.cu, k_trsm.cu).
 //
 // Every mbarrier wait is bounded.  On expiry the thread records an error
 // code in *err, raises the CTA's abort flag, stops issuing work, lets its own
@@ -28,12 +36,15 @@ namespace {
 constexpr int UM = 128;            // tile rows (TMEM lanes)
 constexpr int UN = 128;            // tile columns (TMEM columns)
 constexpr int UKB = 128;           // bytes of k per stage row (one 128-byte swizzle row)
-constexpr int USTAGES = 3;
-constexpr int UT = 128;            // threads: 4 warps
+constexpr int USTAGES = 4;
+constexpr int UEPI = 8;            // epilogue warps
+constexpr int UT = 32 * (2 + UEPI);
 constexpr int kTileBytesA = UM * UKB;
 constexpr int kTileBytesB = UN * UKB;
 constexpr int kStageBytes = kTileBytesA + kTileBytesB;
-constexpr size_t kUmmaSmem = (size_t)USTAGES * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
+constexpr int kScratchFloats = 32 * 33;  // per epilogue warp: one 32 x 32 block, padded
+constexpr size_t kUmmaSmem = (size_t)USTAGES * kStageBytes + sizeof(float) * UEPI * kScratchFloats +
+                             1024 /*align slack*/ + 256 /*barriers*/;
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;
 
@@ -46,6 +57,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
@@ -136,22 +150,24 @@ __host__ __device__ constexpr uint32_t idesc_value() {
 template <bool FP8>
 __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ CUtensorMap map_a,
                                                        const __grid_constant__ CUtensorMap map_b,
-                                                       float* __restrict__ C, int ldc, int m_off, int n_off, int kbytes,
+                                                       float* __restrict__ C, int ldc, int m_off, int n_off,
+                                                       int tiles_n, int tiles, int kbytes,
                                                        const float* __restrict__ scale_a,
                                                        const float* __restrict__ scale_b, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
-    uint8_t* tiles = smem_raw + (base - raw);
-    uint64_t* full = reinterpret_cast<uint64_t*>(tiles + USTAGES * kStageBytes);
+    uint8_t* ring = smem_raw + (base - raw);
+    float* scratch = reinterpret_cast<float*>(ring + USTAGES * kStageBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(scratch + UEPI * kScratchFloats);
     uint64_t* empty = full + USTAGES;
-    uint64_t* done = empty + USTAGES;
+    uint64_t* acc_full = empty + USTAGES;   // [2] MMA -> epilogue
+    uint64_t* acc_empty = acc_full + 2;     // [2] epilogue -> MMA
+    uint64_t* done = acc_empty + 2;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = m_off + blockIdx.y * UM;
-    const int n0 = n_off + blockIdx.x * UN;
     const int KT = kbytes / UKB;
     constexpr int kSteps = UKB / 32;  // 32 bytes of k per MMA: 16 BF16 or 32 E4M3
 
@@ -160,6 +176,10 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], UEPI);
+        }
         mbar_init(done, 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -167,7 +187,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"((uint32_t)UN));
+                     "r"((uint32_t)(2 * UN)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     tc_fence_before();
@@ -175,94 +195,128 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     tc_fence_after();
     const uint32_t tmem = *tmem_slot;
 
-    if (warp == 0 && lane == 0) {
-        // TMA producer.
-        int issued = 0;
-        for (int kt = 0; kt < KT; kt++) {
-            const int s = kt % USTAGES;
-            if (!mbar_wait(&empty[s], ((kt / USTAGES) & 1) ^ 1, abort_flag)) {
-                atomicExch(err, kErrEmptyWait);
-                *abort_flag = 1;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int it = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                const int m0 = m_off + (t / tiles_n) * UM, n0 = n_off + (t % tiles_n) * UN;
+                for (int kt = 0; kt < KT; kt++, it++) {
+                    const int s = it % USTAGES;
+                    if (!mbar_wait(&empty[s], ((it / USTAGES) & 1) ^ 1, abort_flag)) {
+                        atomicExch(err, kErrEmptyWait);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* sa = ring + s * kStageBytes;
+                    mbar_expect_tx(&full[s], kStageBytes);
+                    tma_load_2d(sa, &map_a, &full[s], kt * UKB / (FP8 ? 1 : 2), m0);
+                    tma_load_2d(sa + kTileBytesA, &map_b, &full[s], kt * UKB / (FP8 ? 1 : 2), n0);
+                }
             }
-            uint8_t* sa = tiles + s * kStageBytes;
-            mbar_expect_tx(&full[s], kStageBytes);
-            tma_load_2d(sa, &map_a, &full[s], kt * UKB / (FP8 ? 1 : 2), m0);
-            tma_load_2d(sa + kTileBytesA, &map_b, &full[s], kt * UKB / (FP8 ? 1 : 2), n0);
-            issued = kt + 1;
+            // Let this thread's copies still in flight land before the CTA can exit.
+            for (int j = it - USTAGES < 0 ? 0 : it - USTAGES; j < it; j++) {
+                volatile int no_abort = 0;
+                mbar_wait(&full[j % USTAGES], (j / USTAGES) & 1, &no_abort);
+            }
         }
-        // Let this thread's copies still in flight land before the CTA can exit.
-        for (int kt = issued - USTAGES < 0 ? 0 : issued - USTAGES; kt < issued; kt++) {
-            volatile int no_abort = 0;
-            mbar_wait(&full[kt % USTAGES], (kt / USTAGES) & 1, &no_abort);
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            constexpr uint32_t idesc = idesc_value<FP8>();
+            int it = 0, i = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, i++) {
+                const int b = i & 1;
+                if (!mbar_wait(&acc_empty[b], ((i >> 1) & 1) ^ 1, abort_flag)) {
+                    atomicExch(err, kErrEmptyWait);
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * UN);
+                for (int kt = 0; kt < KT; kt++, it++) {
+                    const int s = it % USTAGES;
+                    if (!mbar_wait(&full[s], (it / USTAGES) & 1, abort_flag)) {
+                        atomicExch(err, kErrFullWait);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(ring + s * kStageBytes);
+                    const uint32_t sb = sa + kTileBytesA;
+#pragma unroll
+                    for (int j = 0; j < kSteps; j++)
+                        umma<FP8>(acc, desc_sw128(sa + 32 * j), desc_sw128(sb + 32 * j), idesc, (kt | j) ? 1u : 0u);
+                    umma_commit(&empty[s]);
+                }
+                if (ok) umma_commit(&acc_full[b]);
+            }
+            umma_commit(done);  // tracks every MMA issued above, also on the abort path
         }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer.
-        constexpr uint32_t idesc = idesc_value<FP8>();
-        int kt = 0;
-        for (; kt < KT; kt++) {
-            const int s = kt % USTAGES;
-            if (!mbar_wait(&full[s], (kt / USTAGES) & 1, abort_flag)) {
-                atomicExch(err, kErrFullWait);
+    } else {  // epilogue
+        const int ew = warp - 2;
+        const int quarter = warp & 3;      // TMEM lanes this warp may read
+        const int half = ew >> 2;          // columns [64 half, 64 half + 64)
+        float* scr = scratch + ew * kScratchFloats;
+        int i = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
+            const int b = i & 1;
+            const int m0 = m_off + (t / tiles_n) * UM, n0 = n_off + (t % tiles_n) * UN;
+            const int r0 = m0 + quarter * 32, c0 = n0 + half * 64;
+            // prefetch this warp's 32 x 64 piece of C, one coalesced row segment per load
+            float cv[2][32];
+#pragma unroll
+            for (int blk = 0; blk < 2; blk++)
+#pragma unroll
+                for (int r = 0; r < 32; r++) cv[blk][r] = C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane];
+            // one decision per warp: tcgen05.ld below is warp-collective
+            const bool got = mbar_wait(&acc_full[b], (i >> 1) & 1, abort_flag);
+            if (!__all_sync(0xffffffffu, got)) {
+                if (lane == 0) atomicExch(err, kErrDoneWait);
                 *abort_flag = 1;
                 break;
             }
             tc_fence_after();
-            const uint32_t sa = smem_u32(tiles + s * kStageBytes);
-            const uint32_t sb = sa + kTileBytesA;
+            const float sc = (scale_a != nullptr) ? scale_a[m0 >> 9] * scale_b[n0 >> 9] : 1.0f;
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * UN + half * 64);
 #pragma unroll
-            for (int j = 0; j < kSteps; j++)
-                umma<FP8>(tmem, desc_sw128(sa + 32 * j), desc_sw128(sb + 32 * j), idesc, (kt | j) ? 1u : 0u);
-            umma_commit(&empty[s]);
+            for (int blk = 0; blk < 2; blk++) {
+                uint32_t a[32];
+                tmem_ld32(taddr + 32 * blk, a);  // lane = tile row, 32 consecutive columns
+                tmem_wait_ld();
+                if (blk == 1) {
+                    // both halves of the accumulator are in registers: hand the buffer back
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&acc_empty[b]);
+                }
+#pragma unroll
+                for (int c = 0; c < 32; c++) scr[lane * 33 + c] = __uint_as_float(a[c]);
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < 32; r++) {
+                    const float v = fmaf(sc, scr[r * 33 + lane], cv[blk][r]);
+                    C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane] = v;
+                }
+                __syncwarp();
+            }
         }
-        umma_commit(done);  // tracks every MMA issued above, also on the abort path
     }
-    __syncwarp();
-
-    // Epilogue: all four warps.  Wait for the accumulator (bounded even when
-    // aborting, so no MMA is in flight when tensor memory is freed).
+    __syncwarp();  // the idle lanes of warps 0 and 1 park here instead of polling beside their worker lane
+    // Wait for every MMA issued (bounded even when aborting) before tensor memory is freed.
     {
         volatile int no_abort = 0;
         if (!mbar_wait(done, 0, &no_abort)) {
-            if (lane == 0) atomicExch(err, kErrDoneWait);
-            *abort_flag = 1;
-        }
-    }
-    tc_fence_after();
-    if (!*abort_flag) {
-        const float sc = (scale_a != nullptr) ? scale_a[m0 >> 9] * scale_b[n0 >> 9] : 1.0f;
-        const int row = m0 + warp * 32 + lane;
-        float* crow = C + (size_t)row * ldc + n0;
-        const uint32_t tbase = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int c0 = 0; c0 < UN; c0 += 64) {
-            float4 cv[16];
-#pragma unroll
-            for (int q = 0; q < 16; q++) cv[q] = *reinterpret_cast<const float4*>(crow + c0 + 4 * q);
-            uint32_t r0[32], r1[32];
-            tmem_ld32(tbase + c0, r0);
-            tmem_ld32(tbase + c0 + 32, r1);
-            tmem_wait_ld();
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                cv[q].x = fmaf(sc, __uint_as_float(r0[4 * q + 0]), cv[q].x);
-                cv[q].y = fmaf(sc, __uint_as_float(r0[4 * q + 1]), cv[q].y);
-                cv[q].z = fmaf(sc, __uint_as_float(r0[4 * q + 2]), cv[q].z);
-                cv[q].w = fmaf(sc, __uint_as_float(r0[4 * q + 3]), cv[q].w);
-                cv[q + 8].x = fmaf(sc, __uint_as_float(r1[4 * q + 0]), cv[q + 8].x);
-                cv[q + 8].y = fmaf(sc, __uint_as_float(r1[4 * q + 1]), cv[q + 8].y);
-                cv[q + 8].z = fmaf(sc, __uint_as_float(r1[4 * q + 2]), cv[q + 8].z);
-                cv[q + 8].w = fmaf(sc, __uint_as_float(r1[4 * q + 3]), cv[q + 8].w);
-            }
-#pragma unroll
-            for (int q = 0; q < 16; q++) *reinterpret_cast<float4*>(crow + c0 + 4 * q) = cv[q];
+            if (threadIdx.x == 0) atomicExch(err, kErrDoneWait);
         }
     }
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)UN));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * UN)));
     }
 }
 
@@ -331,11 +385,17 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     CUtensorMap ma, mb;
     LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8));
     LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8));
-    const dim3 grid(n / UN, m / UM);
+    const int tiles_n = n / UN, tiles = tiles_n * (m / UM);
+    int dev = 0, sms = 0;
+    LP_CUDA(cudaGetDevice(&dev));
+    LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int grid = tiles < sms ? tiles : sms;
     if (fp8)
-        k_umma_update<true><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, kbytes, scale_a, scale_b, err);
+        k_umma_update<true><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles, kbytes, scale_a,
+                                                         scale_b, err);
     else
-        k_umma_update<false><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, kbytes, nullptr, nullptr, err);
+        k_umma_update<false><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles, kbytes,
+                                                          nullptr, nullptr, err);
     count_launch();
     LP_CUDA(cudaGetLastError());
     return LP_OK;
