@@ -1,6 +1,7 @@
 // C ABI of liblpcuda.so (declared in include/lpcuda.h): context, workspace,
 // the block-step schedule of the factorization, the substitution, and the
 // host entry points that stand in for the reference's execution backend.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -79,6 +80,11 @@ int prof_begin(lp_ctx* c, cudaStream_t st) {
             c->prof_ev.push_back(e);
         }
     }
+    if (!c->base_recorded) {
+        if (c->prof_base == nullptr) LP_CUDA(cudaEventCreate(&c->prof_base));
+        LP_CUDA(cudaEventRecord(c->prof_base, st));
+        c->base_recorded = true;
+    }
     const int e0 = (int)c->prof_used++;
     LP_CUDA(cudaEventRecord(c->prof_ev[e0], st));
     return e0;
@@ -88,7 +94,7 @@ int prof_end(lp_ctx* c, cudaStream_t st, int kind, int e0, double flops, double 
     if (e0 < 0) return LP_OK;
     const int e1 = (int)c->prof_used++;
     LP_CUDA(cudaEventRecord(c->prof_ev[e1], st));
-    c->marks.push_back(StageMark{kind, e0, e1, flops, bytes});
+    c->marks.push_back(StageMark{kind, st == c->aux ? 1 : (st == c->aux2 ? 2 : 0), e0, e1, flops, bytes});
     return LP_OK;
 }
 
@@ -96,9 +102,14 @@ int prof_end(lp_ctx* c, cudaStream_t st, int kind, int e0, double flops, double 
 static int prof_collect(lp_ctx* c) {
     if (c->marks.empty()) return LP_OK;
     LP_CUDA(cudaStreamSynchronize(c->stream));
+    LP_CUDA(cudaStreamSynchronize(c->aux));
+    LP_CUDA(cudaStreamSynchronize(c->aux2));
     for (const auto& m : c->marks) {
-        float ms = 0.0f;
+        float ms = 0.0f, a = 0.0f, b = 0.0f;
         LP_CUDA(cudaEventElapsedTime(&ms, c->prof_ev[m.e0], c->prof_ev[m.e1]));
+        LP_CUDA(cudaEventElapsedTime(&a, c->prof_base, c->prof_ev[m.e0]));
+        LP_CUDA(cudaEventElapsedTime(&b, c->prof_base, c->prof_ev[m.e1]));
+        c->timeline.push_back(lp_stage_event{m.kind, m.stream, a * 1e-3, b * 1e-3});
         c->prof_s[m.kind] += ms * 1e-3;
         c->prof_flops[m.kind] += m.flops;
         c->prof_bytes[m.kind] += m.bytes;
@@ -128,8 +139,13 @@ static int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
         LP_CHECK(launch_lu_small(dd, lda, ib, st));
         const int r = bs - (kk + 1) * ib;
         if (r <= 0) break;
+        // top on st, left beside it on aux2 (both read only the factored block)
+        LP_CUDA(cudaEventRecord(c->ev_side, st));
+        LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
         LP_CHECK(launch_trsm_top(dd, lda, dd + ib, lda, ib, r, st));
-        LP_CHECK(launch_trsm_left(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, st));
+        LP_CHECK(launch_trsm_left(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, c->aux2));
+        LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
+        LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
         LP_CHECK(launch_sgemm_update(dd + (size_t)ib * lda + ib, lda, lti, r, dd + ib, lda, r, r, ib, st));
     }
     return LP_OK;
@@ -189,12 +205,18 @@ int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cu
     const int rest = n - (K + 1) * bs;
     if (rest <= 0) return LP_OK;
     const double r = rest;
+    // top on st and left on aux2 run concurrently: both read only the factored
+    // diagonal block and write disjoint blocks (top uses st's dsub slot, left Lt)
+    LP_CUDA(cudaEventRecord(c->ev_side, st));
+    LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
+    e = prof_begin(c, c->aux2);
+    LP_CHECK(left_blocked(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, c->aux2));
+    LP_CHECK(prof_end(c, c->aux2, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
+    LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
     e = prof_begin(c, st);
     LP_CHECK(top_blocked(c, d, lda, d + bs, lda, bs, rest, st));
     LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, trsm_flops(b, r), 8.0 * b * r));
-    e = prof_begin(c, st);
-    LP_CHECK(left_blocked(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
-    LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
+    LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
     return LP_OK;
 }
 
@@ -331,6 +353,9 @@ int lp_ctx_create(int device, lp_ctx** out) {
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->aux, cudaStreamNonBlocking, prio_hi);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->aux2, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_side, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_side_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_block, cudaEventDisableTiming | cudaEventBlockingSync);
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
@@ -346,11 +371,15 @@ int lp_ctx_destroy(lp_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream != nullptr) cudaStreamSynchronize(c->stream);
     if (c->aux != nullptr) cudaStreamSynchronize(c->aux);
+    if (c->aux2 != nullptr) cudaStreamSynchronize(c->aux2);
     c->release_all();
     for (int i = 0; i < 8; i++)
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
     if (c->ev_fork != nullptr) cudaEventDestroy(c->ev_fork);
     if (c->ev_join != nullptr) cudaEventDestroy(c->ev_join);
+    if (c->ev_side != nullptr) cudaEventDestroy(c->ev_side);
+    if (c->ev_side_done != nullptr) cudaEventDestroy(c->ev_side_done);
+    if (c->aux2 != nullptr) cudaStreamDestroy(c->aux2);
     if (c->ev_block != nullptr) cudaEventDestroy(c->ev_block);
     if (c->aux != nullptr) cudaStreamDestroy(c->aux);
     if (c->stream != nullptr) cudaStreamDestroy(c->stream);
@@ -398,6 +427,21 @@ int lp_ctx_read_profile(lp_ctx* c, lp_profile* out, int reset) {
         }
     }
     out->kernel_launches = launch_count();
+    if (reset) {
+        c->timeline.clear();
+        c->base_recorded = false;
+    }
+    return LP_OK;
+}
+
+int lp_ctx_read_timeline(lp_ctx* c, lp_stage_event* out, int max, int* count) {
+    if (c == nullptr || out == nullptr || count == nullptr || max < 0)
+        return fail(LP_E_INVALID, "lp_ctx_read_timeline: bad argument");
+    LP_CUDA(cudaSetDevice(c->device));
+    LP_CHECK(prof_collect(c));
+    const int k = (int)std::min<size_t>((size_t)max, c->timeline.size());
+    for (int i = 0; i < k; i++) out[i] = c->timeline[i];
+    *count = k;
     return LP_OK;
 }
 

@@ -10,6 +10,7 @@ namespace lp {
 // One profiled stage launch: events e0/e1 of the context's pool bracket it.
 struct StageMark {
     int kind;
+    int stream;  // 0: the context's main stream, 1: its auxiliary stream
     int e0, e1;
     double flops, bytes;
 };
@@ -65,6 +66,8 @@ struct lp_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t aux = nullptr;               // second (high-priority) stream for concurrent panel work
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t aux2 = nullptr;              // third stream: the left update runs here beside the top update
+    cudaEvent_t ev_side = nullptr, ev_side_done = nullptr;
     cudaEvent_t ev_block = nullptr;           // blocking-sync event: waits yield the CPU instead of spinning
     cudaEvent_t ev[8] = {nullptr};
     lp::Workspace lt;    // transposed left panels (2 x bs x n, alternating by block step)
@@ -90,6 +93,9 @@ struct lp_ctx {
     std::vector<cudaEvent_t> prof_ev;         // event pool, reused after every read
     size_t prof_used = 0;
     std::vector<lp::StageMark> marks;
+    std::vector<lp_stage_event> timeline;     // collected marks, relative to prof_base
+    cudaEvent_t prof_base = nullptr;
+    bool base_recorded = false;
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
@@ -100,6 +106,8 @@ struct lp_ctx {
         bgraph = nullptr;
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();
+        if (prof_base != nullptr) cudaEventDestroy(prof_base);
+        prof_base = nullptr;
         if (hnorm != nullptr) cudaFreeHost(hnorm);
         hnorm = nullptr;
         hnorm_cap = 0;

@@ -58,6 +58,11 @@ class LpProfile(ctypes.Structure):
         return d
 
 
+class LpStageEvent(ctypes.Structure):
+    _fields_ = [("stage", ctypes.c_int), ("stream", ctypes.c_int), ("t0_s", ctypes.c_double),
+                ("t1_s", ctypes.c_double)]
+
+
 class LpSystem(ctypes.Structure):
     _fields_ = [("n", ctypes.c_int), ("nrhs", ctypes.c_int), ("lda", ctypes.c_int), ("ldb", ctypes.c_int),
                 ("a_off", ctypes.c_longlong), ("b_off", ctypes.c_longlong)]
@@ -149,6 +154,7 @@ def lib() -> ctypes.CDLL:
     L.lp_ctx_device_name.argtypes = [_VP, ctypes.c_char_p, _I]
     L.lp_ctx_set_profiling.argtypes = [_VP, _I]
     L.lp_ctx_read_profile.argtypes = [_VP, ctypes.POINTER(LpProfile), _I]
+    L.lp_ctx_read_timeline.argtypes = [_VP, ctypes.POINTER(LpStageEvent), _I, ctypes.POINTER(_I)]
     L.lp_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(_VP)]
     L.lp_host_free.argtypes = [_VP]
     L.lp_lu_block_dev.argtypes = [_VP, _VP, _I, _I]
@@ -275,6 +281,13 @@ class Context:
 
     def set_profiling(self, on: bool) -> None:
         check(lib().lp_ctx_set_profiling(self._h, int(on)), "lp_ctx_set_profiling")
+
+    def read_timeline(self, max_events: int = 1 << 16) -> list[tuple]:
+        """(stage, stream, t0_s, t1_s) of every profiled stage launch since the last reset."""
+        out = (LpStageEvent * max_events)()
+        k = _I(0)
+        check(lib().lp_ctx_read_timeline(self._h, out, max_events, ctypes.byref(k)), "lp_ctx_read_timeline")
+        return [(STAGES[out[i].stage], out[i].stream, out[i].t0_s, out[i].t1_s) for i in range(k.value)]
 
     def read_profile(self, reset: bool = True) -> dict:
         p = LpProfile()

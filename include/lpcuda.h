@@ -108,8 +108,20 @@ typedef struct {
     long long kernel_launches;       /* kernels launched through this library by the process (cumulative) */
 } lp_profile;
 int lp_ctx_set_profiling(lp_ctx* ctx, int on);
-/* Waits for the context's stream, fills out, and clears the stage sums if reset. */
+/* Waits for the context's streams, fills out, and clears the stage sums (and
+ * the timeline below) if reset. */
 int lp_ctx_read_profile(lp_ctx* ctx, lp_profile* out, int reset);
+/* One profiled stage launch: when it started and ended on the device, in
+ * seconds after the first stage recorded since the last reset, and on which
+ * stream (0: the context's main stream, 1: its auxiliary stream, where the
+ * look-ahead panel runs). */
+typedef struct {
+    int stage;                       /* LP_STAGE_* */
+    int stream;
+    double t0_s, t1_s;
+} lp_stage_event;
+/* Copies up to max entries of the stage timeline into out (*count of them). */
+int lp_ctx_read_timeline(lp_ctx* ctx, lp_stage_event* out, int max, int* count);
 
 /* ---- block stages (device pointers) -------------------------------------
  * The four kernels of LINPACK/src/device/hpl_torus_PCIE.cl, as whole-panel
