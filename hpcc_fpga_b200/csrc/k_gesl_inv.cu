@@ -11,9 +11,23 @@
 //                              triangle, the U factor of M).
 // Within a block the forward sweep is then y = Y^T acc and the backward sweep
 // s = X^T acc, x = -s: a 128 x 128 matrix-vector product over all 256 threads
-// instead of a 128-step sequential chain.  Blocks are still visited in order,
-// one launch per block and direction; step (b), the update of the remaining
-// unknowns with the block's row panel, is the shared panel_gemv.
+// instead of a 128-step sequential chain.
+//
+// Each sweep is ONE persistent launch over 128-unknown tiles.  A CTA takes
+// tiles in ticket order (atomic counter: forward 0, 1, 2, ...; backward from
+// the last tile down) and accumulates, for its tile j, the contributions of
+// every earlier tile K: acc_j += y_K^T * S[rows of K][columns of j], reading
+// each factor element once.  It loads the factor rows of tile K before
+// waiting for K's "solved" flag, so the wait overlaps the memory traffic, and
+// keeps per-thread partial sums until all K are in; then it reduces them,
+// forms y_j with the block operator (prefetched into shared memory when the
+// tile started), publishes y_j and raises flag j.  A CTA only waits on tiles
+// taken before its own by running CTAs, so progress is guaranteed; every wait
+// is bounded nonetheless, and a CTA that gives up records the error, writes
+// NaN for its tile (the result then fails every residual check) and still
+// raises its flag so no other CTA waits on it.
+#include <algorithm>
+
 #include "gesl_common.cuh"
 
 namespace lp {
@@ -141,10 +155,10 @@ __global__ void __launch_bounds__(256) k_inv_left(const float* __restrict__ a, i
     }
 }
 
-// coef[r][i] = sum_k M[k][i] * acc[r][k] for the block at k0 (M = Y or X of
-// that block); all 256 threads: thread (h, i) sums k in [64h, 64h+64).
+// coef[r][i] = sum_k M[k][i] * acc[r][k] for a 128 x 128 operator M (shared
+// memory); all 256 threads: thread (h, i) sums k in [64h, 64h+64).
 template <int NR>
-__device__ __forceinline__ void block_matvec(const float* __restrict__ M, const float* acc, float* part, float* coef) {
+__device__ __forceinline__ void block_matvec(const float* M, const float* acc, float* part, float* coef) {
     const int i = threadIdx.x & (SB - 1), h = threadIdx.x >> 7;
     float p[NR];
 #pragma unroll
@@ -166,86 +180,186 @@ __device__ __forceinline__ void block_matvec(const float* __restrict__ M, const 
     __syncthreads();
 }
 
-template <int NR>
-__device__ __forceinline__ void load_acc(float* acc, const float* __restrict__ w, int ldw, int nrhs, int k0, int kb) {
-    for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
-        const int r = idx / SB, i = idx - r * SB;
-        acc[idx] = (r < nrhs && i < kb) ? w[(size_t)r * ldw + k0 + i] : 0.0f;
+constexpr int kSpinLimit = 1 << 22;  // x ~100 ns per poll: well under a second
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Lane 0 of the calling warp polls flag f (bounded); the warp then proceeds
+// together.  false: the wait gave up or another CTA aborted (err set).
+__device__ __forceinline__ bool warp_wait_flag(const int* f, int* err) {
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) {
+        ok = 0;
+        for (int it = 0; it < kSpinLimit; it++) {
+            if (ld_acquire(f) != 0) {
+                ok = 1;
+                break;
+            }
+            if (*(volatile int*)err != 0) break;
+            __nanosleep(64);
+        }
+        if (!ok) atomicExch(err, 1);
     }
-    __syncthreads();
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
 }
 
-template <int NR>
-__global__ void __launch_bounds__(GT) k_gesl_fwd_inv(const float* __restrict__ a, int lda, int n,
-                                                     const float* __restrict__ inv, float* __restrict__ w1,
-                                                     float* __restrict__ w2, int ldw, int nrhs, int k0) {
-    extern __shared__ float smem[];
-    float* red = smem;                       // 8 x NR x 128 (panel_gemv)
-    float* acc = red + 8 * NR * SB;          // NR x 128
-    float* part = acc + NR * SB;             // 2 x NR x 128
-    float* ys = part + 2 * NR * SB;          // NR x 128
-    const int kb = min(SB, n - k0);
-    load_acc<NR>(acc, w1, ldw, nrhs, k0, kb);
-    block_matvec<NR>(inv + (size_t)(k0 / SB) * 2 * BLK2 + BLK2, acc, part, ys);
-    if (blockIdx.x == 0)
-        for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
-            const int r = idx / SB, i = idx - r * SB;
-            if (r < nrhs && i < kb) w2[(size_t)r * ldw + k0 + i] = ys[idx];
-        }
-    const int col0 = k0 + kb + blockIdx.x * GCOLS;
-    if (col0 < n) panel_gemv<NR>(a, lda, k0, kb, col0, n, ys, red, w1, ldw, nrhs);
-}
-
-template <int NR>
-__global__ void __launch_bounds__(GT) k_gesl_bwd_inv(const float* __restrict__ a, int lda, int n,
-                                                     const float* __restrict__ inv, float* __restrict__ w2,
-                                                     float* __restrict__ out, int ldo, int ldw, int nrhs, int k0) {
-    extern __shared__ float smem[];
-    float* red = smem;
-    float* acc = red + 8 * NR * SB;
-    float* part = acc + NR * SB;
-    float* ss = part + 2 * NR * SB;
-    const int kb = min(SB, n - k0);
-    load_acc<NR>(acc, w2, ldw, nrhs, k0, kb);
-    block_matvec<NR>(inv + (size_t)(k0 / SB) * 2 * BLK2, acc, part, ss);
-    if (blockIdx.x == 0)
-        for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
-            const int r = idx / SB, i = idx - r * SB;
-            if (r < nrhs && i < kb) out[(size_t)r * ldo + k0 + i] = -ss[idx];
-        }
-    const int col0 = blockIdx.x * GCOLS;
-    if (col0 < k0) panel_gemv<NR>(a, lda, k0, kb, col0, k0, ss, red, w2, ldw, nrhs);
-}
-
-template <int NR>
-constexpr size_t inv_smem() {
-    return sizeof(float) * (8 * NR + 4 * NR) * (size_t)SB;
-}
-
-template <int NR>
-int sweeps_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* w1, float* w2, const float* inv,
-               cudaStream_t st) {
+// The persistent sweep.  FWD: tiles ascend, acc_j = b_j + sum_{K<j} y_K S[K][j],
+// y_j = Y_j^T acc_j -> w (ldw).  Backward: tiles descend,
+// acc_j = y_j + sum_{K>j} s_K S[K][j], s_j = X_j^T acc_j -> w (ldw), x_j = -s_j -> out.
+// in: b (forward) / y (backward), leading dimension ldi.
+template <int NR, bool FWD>
+__global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, int lda, int n,
+                                                   const float* __restrict__ inv, const float* __restrict__ in,
+                                                   int ldi, const float* __restrict__ wprev, float* __restrict__ w,
+                                                   int ldw, float* __restrict__ out, int ldo, int nrhs,
+                                                   int* __restrict__ flags, int* __restrict__ ticket,
+                                                   int* __restrict__ err) {
+    extern __shared__ __align__(16) float smem[];
+    float* op = smem;                 // 128 x 128 block operator
+    float* red = op + BLK2;           // 8 x NR x 128 partial sums
+    float* acc = red + 8 * NR * SB;   // NR x 128
+    float* part = acc + NR * SB;      // 2 x NR x 128
+    float* res = part + 2 * NR * SB;  // NR x 128
+    __shared__ int s_tile;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (n + SB - 1) / SB;
-    for (int K = 0; K < nblk; K++) {
-        const int k0 = K * SB;
-        const int rest = n - k0 - min(SB, n - k0);
-        const int grid = rest > 0 ? (rest + GCOLS - 1) / GCOLS : 1;
-        k_gesl_fwd_inv<NR><<<grid, GT, inv_smem<NR>(), st>>>(a, lda, n, inv, w1, w2, n, nrhs, k0);
+    for (;;) {
+        __syncthreads();  // the previous tile's shared data is consumed
+        if (tid == 0) s_tile = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int t = s_tile;
+        if (t >= nblk) break;
+        const int j = FWD ? t : nblk - 1 - t;
+        const int c0 = j * SB, kb = min(SB, n - c0);
+        // the tile's block operator (Y for the forward sweep, X backward), 16-byte copies
+        {
+            const float* src = inv + (size_t)j * 2 * BLK2 + (FWD ? BLK2 : 0);
+            for (int idx = tid; idx < BLK2 / 4; idx += GT) {
+                const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(op + 4 * idx));
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 4 * idx) : "memory");
+            }
+            asm volatile("cp.async.commit_group;\n" ::: "memory");
+        }
+        // partial sums of this thread: columns c0 + 4 lane .. +3, rows 16 warp .. +15 of every source tile
+        float p[NR][4];
+#pragma unroll
+        for (int q = 0; q < NR; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) p[q][e] = 0.0f;
+        const int col = c0 + 4 * lane;
+        const bool vec = col + 3 < n;
+        bool ok = true;
+        const int nsrc = FWD ? j : nblk - 1 - j;
+        for (int s = 0; s < nsrc; s++) {
+            const int K = FWD ? s : nblk - 1 - s;
+            const int k0 = K * SB, kbK = min(SB, n - k0);
+            float4 v[16];
+#pragma unroll
+            for (int r = 0; r < 16; r++) {
+                const int row = 16 * warp + r;
+                const float* src = a + (size_t)(k0 + row) * lda + col;
+                if (row < kbK && vec) {
+                    v[r] = *reinterpret_cast<const float4*>(src);
+                } else {
+                    v[r].x = (row < kbK && col < n) ? src[0] : 0.0f;
+                    v[r].y = (row < kbK && col + 1 < n) ? src[1] : 0.0f;
+                    v[r].z = (row < kbK && col + 2 < n) ? src[2] : 0.0f;
+                    v[r].w = (row < kbK && col + 3 < n) ? src[3] : 0.0f;
+                }
+            }
+            if (!warp_wait_flag(&flags[K], err)) {
+                ok = false;
+                break;
+            }
+#pragma unroll
+            for (int r = 0; r < 16; r++) {
+                const int row = 16 * warp + r;
+#pragma unroll
+                for (int q = 0; q < NR; q++) {
+                    // written by another CTA after this CTA may have cached the line: read through L2
+                    const float yk = (q < nrhs && row < kbK) ? __ldcg(wprev + (size_t)q * ldw + k0 + row) : 0.0f;
+                    p[q][0] = fmaf(yk, v[r].x, p[q][0]);
+                    p[q][1] = fmaf(yk, v[r].y, p[q][1]);
+                    p[q][2] = fmaf(yk, v[r].z, p[q][2]);
+                    p[q][3] = fmaf(yk, v[r].w, p[q][3]);
+                }
+            }
+        }
+        ok = __syncthreads_and(ok);
+#pragma unroll
+        for (int q = 0; q < NR; q++)
+#pragma unroll
+            for (int e = 0; e < 4; e++) red[(warp * NR + q) * SB + 4 * lane + e] = p[q][e];
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncthreads();
+        for (int idx = tid; idx < NR * SB; idx += GT) {
+            const int q = idx / SB, i = idx - q * SB;
+            float v = 0.0f;
+            if (q < nrhs && i < kb) {
+                v = in[(size_t)q * ldi + c0 + i];
+#pragma unroll
+                for (int ww = 0; ww < GT / 32; ww++) v += red[(ww * NR + q) * SB + i];
+            }
+            acc[idx] = v;
+        }
+        __syncthreads();
+        block_matvec<NR>(op, acc, part, res);
+        for (int idx = tid; idx < NR * SB; idx += GT) {
+            const int q = idx / SB, i = idx - q * SB;
+            if (q < nrhs && i < kb) {
+                const float v = ok ? res[idx] : __int_as_float(0x7fc00000);  // NaN marks an aborted solve
+                w[(size_t)q * ldw + c0 + i] = v;
+                if (!FWD) out[(size_t)q * ldo + c0 + i] = -v;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) st_release(&flags[j], 1);
     }
-    for (int K = nblk - 1; K >= 0; K--) {
-        const int k0 = K * SB;
-        const int grid = k0 > 0 ? (k0 + GCOLS - 1) / GCOLS : 1;
-        k_gesl_bwd_inv<NR><<<grid, GT, inv_smem<NR>(), st>>>(a, lda, n, inv, w2, b, ldb, n, nrhs, k0);
-    }
-    count_launch(2 * nblk);
+}
+
+template <int NR>
+constexpr size_t sweep_smem() {
+    return sizeof(float) * ((size_t)BLK2 + (8 * NR + 4 * NR) * (size_t)SB);
+}
+
+template <int NR>
+int sweeps(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* w1, float* w2, const float* inv,
+           int* sync, int sms, cudaStream_t st) {
+    const int nblk = (n + SB - 1) / SB;
+    int* flags_f = sync;
+    int* flags_b = sync + nblk;
+    int* tickets = sync + 2 * nblk;
+    int* err = tickets + 2;
+    LP_CUDA(cudaMemsetAsync(sync, 0, sizeof(int) * (2 * (size_t)nblk + 2), st));  // the error word persists
+    const int per_sm = NR >= 16 ? 1 : 2;
+    const int grid = std::min(nblk, per_sm * sms);
+    // forward: b -> y (w2)
+    k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, b, ldb, w2, w2, n, nullptr, 0, nrhs,
+                                                              flags_f, tickets, err);
+    // backward: y (w2) -> s (w1), x -> b
+    k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, w2, n, w1, w1, n, b, ldb, nrhs,
+                                                               flags_b, tickets + 1, err);
+    count_launch(2);
     LP_CUDA(cudaGetLastError());
     return LP_OK;
 }
 
 template <int NR>
 int inv_attrs() {
-    LP_CUDA(cudaFuncSetAttribute(k_gesl_fwd_inv<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem<NR>()));
-    LP_CUDA(cudaFuncSetAttribute(k_gesl_bwd_inv<NR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem<NR>()));
+    LP_CUDA(cudaFuncSetAttribute(k_gesl_sweep<NR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem<NR>()));
+    LP_CUDA(cudaFuncSetAttribute(k_gesl_sweep<NR, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sweep_smem<NR>()));
     return LP_OK;
 }
 
@@ -274,23 +388,29 @@ int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_
     return LP_OK;
 }
 
-// Forward + back substitution with precomputed block inverses.
+// Sync words of the persistent sweeps: flags of both directions, two tickets, an error word.
+size_t gesl_sync_ints(int n) { return 2 * (size_t)((n + SB - 1) / SB) + 3; }
+
+// Forward + back substitution with precomputed block inverses; sync: gesl_sync_ints(n)
+// zero-initialised ints whose last one is the error word (non-zero after a wait gave up).
 int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
-                    cudaStream_t st) {
+                    int* sync, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return LP_OK;
+    if (lda % 4 != 0 || !aligned16(a)) return fail(LP_E_INVALID, "gesl: factors need lda % 4 == 0, 16-byte aligned");
+    int dev = 0, sms = 0;
+    LP_CUDA(cudaGetDevice(&dev));
+    LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
         const int g = (nrhs - r0) < 16 ? (nrhs - r0) : 16;
         float* bb = b + (size_t)r0 * ldb;
         float* w1 = work;
         float* w2 = work + (size_t)n * g;
-        LP_CUDA(cudaMemcpy2DAsync(w1, sizeof(float) * n, bb, sizeof(float) * ldb, sizeof(float) * n, g,
-                                  cudaMemcpyDeviceToDevice, st));
         if (g == 1)
-            LP_CHECK(sweeps_inv<1>(a, lda, n, bb, ldb, g, w1, w2, inv, st));
+            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
         else if (g <= 4)
-            LP_CHECK(sweeps_inv<4>(a, lda, n, bb, ldb, g, w1, w2, inv, st));
+            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
         else
-            LP_CHECK(sweeps_inv<16>(a, lda, n, bb, ldb, g, w1, w2, inv, st));
+            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
     }
     return LP_OK;
 }

@@ -270,12 +270,16 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
 }
 
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st) {
-    LP_CHECK(c->gw.ensure(sizeof(float) * gesl_work_floats(n, nrhs)));
+    const size_t wf = gesl_work_floats(n, nrhs), si = gesl_sync_ints(n);
+    LP_CHECK(c->gw.ensure(sizeof(float) * wf + sizeof(int) * si));
     LP_CHECK(c->ginv.ensure(sizeof(float) * gesl_inv_floats(n)));
     float* inv = static_cast<float*>(c->ginv.ptr);
+    float* work = static_cast<float*>(c->gw.ptr);
+    int* sync = reinterpret_cast<int*>(work + wf);
+    LP_CUDA(cudaMemsetAsync(sync + si - 1, 0, sizeof(int), st));  // error word of the sweeps
     const int e = prof_begin(c, st);
     LP_CHECK(launch_diag_inverses(dLU, lda, n, inv, st));
-    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, static_cast<float*>(c->gw.ptr), inv, st));
+    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, work, inv, sync, st));
     const double nn = n;
     return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
 }
