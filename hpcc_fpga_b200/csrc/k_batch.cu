@@ -16,10 +16,10 @@
 //     size bucket, chosen by the autotuner): the diagonal block factored by
 //     one warp in registers (pivots and columns by shuffles); the top block
 //     row (column-independent) and left block column (row-independent) by
-//     their recurrences in registers; the trailing update per 64-row block,
+//     their recurrences in registers; the trailing update per 128-row block,
 //     its left panel resident in shared memory, the 64-column top tiles
-//     streamed through a cp.async double buffer and C accumulated in
-//     registers.  (Panel widths 16 and 32 keep a recurrence in registers.)
+//     streamed in with cp.async one tile ahead, each thread's 8 x 4 piece of
+//     C loaded into registers while its products run.  (Panel widths 16 and 32 keep a recurrence in registers.)
 //     Then blocked forward/back sweeps with the right-hand sides resident in
 //     shared memory and each diagonal block staged before its sequential solve.
 // Arithmetic uses fused multiply-add: results agree with the reference to
@@ -32,7 +32,6 @@ namespace {
 constexpr int BT = 256;
 constexpr int SMALL_MAX = 128;
 constexpr int RHS_MAX = 16;
-constexpr int TILE = 64;
 constexpr int NBUCKETS = 5;
 // Flag in BatchSys::nrhs (server use only; the public entry points accept
 // nrhs <= 16): the matrix already holds its factors, solve only.
@@ -53,6 +52,8 @@ struct Tune {
 constexpr size_t kSmallFloats = (size_t)SMALL_MAX * (SMALL_MAX + 1) + (size_t)RHS_MAX * SMALL_MAX;
 constexpr size_t kBlockedFloats = (size_t)RHS_MAX * 1024;  // right-hand sides of n <= 1024 in the solve phase
 constexpr size_t kBatchSmem = sizeof(float) * (kSmallFloats > kBlockedFloats ? kSmallFloats : kBlockedFloats);
+// factor_blocked<32>: diagonal block, left panel (128 rows), 2 top tiles
+static_assert(sizeof(float) * (32 * 33 + 32 * 132 + 2 * 32 * 64) <= kBatchSmem, "blocked smem");
 
 __device__ __forceinline__ int bucket_of(int n) {
     return n <= 64 ? 0 : n <= 128 ? 1 : n <= 256 ? 2 : n <= 512 ? 3 : 4;
@@ -145,48 +146,49 @@ __device__ __noinline__ void solve_small(float* a, int lda, int n, float* b, int
 // into the persistent loop its register array is not fully unrolled.
 template <int NB, int DL>
 __device__ __noinline__ void warp_diag_lu(float* d, int lda, int kb, float* Ds) {
+    // A partial last block is padded with the identity: diag(D, I) factors as
+    // diag(LU_D, I), so every step runs unconditionally (no per-step branches
+    // between the shuffles) and only the kb x kb part is written back.
     const int lane = threadIdx.x & 31;
-    const bool act = lane < kb;
     float x[NB];
 #pragma unroll
-    for (int j = 0; j < NB; j++) x[j] = (act && j < kb) ? d[(size_t)j * lda + lane] : 0.0f;
+    for (int j = 0; j < NB; j++)
+        x[j] = (lane < kb && j < kb) ? d[(size_t)j * lda + lane] : (j == lane ? 1.0f : 0.0f);
 #pragma unroll
     for (int k = 0; k < NB; k++) {
-        if (k < kb) {
-            const float inv = (float)(-1.0 / (double)__shfl_sync(0xffffffffu, x[k], k));
-            if (lane > k)
-                x[k] *= inv;
-            else if (lane == k)
-                x[k] = inv;
+        // -1/pivot correctly rounded in float (equal to the double quotient rounded to float)
+        const float inv = -__frcp_rn(__shfl_sync(0xffffffffu, x[k], k));
+        if (lane > k)
+            x[k] *= inv;
+        else if (lane == k)
+            x[k] = inv;
 #pragma unroll
-            for (int j = k + 1; j < NB; j++) {
-                if (j < kb) {
-                    const float sjk = __shfl_sync(0xffffffffu, x[j], k);
-                    if (lane > k) x[j] = fmaf(x[k], sjk, x[j]);
-                }
-            }
+        for (int j = k + 1; j < NB; j++) {
+            const float sjk = __shfl_sync(0xffffffffu, x[j], k);
+            if (lane > k) x[j] = fmaf(x[k], sjk, x[j]);
         }
     }
-    if (act) {
+    if (lane < NB) {
 #pragma unroll
-        for (int j = 0; j < NB; j++)
-            if (j < kb) {
-                d[(size_t)j * lda + lane] = x[j];
-                Ds[j * DL + lane] = x[j];
-            }
+        for (int j = 0; j < NB; j++) {
+            Ds[j * DL + lane] = x[j];
+            if (lane < kb && j < kb) d[(size_t)j * lda + lane] = x[j];
+        }
     }
 }
 
 // Blocked factorization of one system in global memory (see file comment).
-// Trailing update per row block of TILE rows: the block's left panel (k-major)
-// stays in shared memory, the top tiles stream through a cp.async double
-// buffer, and each thread keeps its 4 x 4 piece of C in registers.
+// Trailing update per row block of 128 rows: the block's left panel (k-major)
+// stays in shared memory, the 64-column top tiles stream through a cp.async
+// double buffer, and each thread loads its 8 x 4 piece of C into registers
+// before the rank-NB products, which hide the load.
 template <int NB>
 __device__ __noinline__ void factor_blocked(float* a, int lda, int n, float* sm) {
-    constexpr int DL = NB + 1, LS = TILE + 4;
+    constexpr int TM = 128, TN = 64;   // trailing-update tile
+    constexpr int DL = NB + 1, LS = TM + 4;
     float* Ds = sm;                    // NB x DL diagonal block
     float* Lt = Ds + NB * DL;          // NB x LS: left panel of one row block, k-major
-    float* Tb = Lt + NB * LS;          // 2 x NB x TILE: top tiles
+    float* Tb = Lt + NB * LS;          // 2 x NB x TN: top tiles
     const int tid = threadIdx.x;
     for (int k0 = 0; k0 < n; k0 += NB) {
         const int kb = min(NB, n - k0);
@@ -195,135 +197,167 @@ __device__ __noinline__ void factor_blocked(float* a, int lda, int n, float* sm)
         if (tid < 32) warp_diag_lu<NB, DL>(d, lda, kb, Ds);
         __syncthreads();
         if (rem <= 0) break;
+        // (rem > 0: this block is full, kb == NB)
         // top: every column c of the block row, t_k *= D_kk; t_j += t_k D_jk (j > k)
         for (int c = r0 + tid; c < n; c += BT) {
             float x[NB];
 #pragma unroll
-            for (int i = 0; i < NB; i++) x[i] = (i < kb) ? a[(size_t)(k0 + i) * lda + c] : 0.0f;
+            for (int i = 0; i < NB; i++) x[i] = a[(size_t)(k0 + i) * lda + c];
 #pragma unroll
             for (int k = 0; k < NB; k++) {
-                if (k < kb) {
-                    const float xk = x[k] * Ds[k * DL + k];
-                    x[k] = xk;
+                const float xk = x[k] * Ds[k * DL + k];
+                x[k] = xk;
 #pragma unroll
-                    for (int j = k + 1; j < NB; j++) x[j] = fmaf(xk, Ds[j * DL + k], x[j]);
-                }
+                for (int j = k + 1; j < NB; j++) x[j] = fmaf(xk, Ds[j * DL + k], x[j]);
             }
 #pragma unroll
-            for (int i = 0; i < NB; i++)
-                if (i < kb) a[(size_t)(k0 + i) * lda + c] = x[i];
+            for (int i = 0; i < NB; i++) a[(size_t)(k0 + i) * lda + c] = x[i];
         }
         // left: every row rr of the block column, l_i += l_k D_ki (i > k)
+        const bool vec = ((lda & 3) == 0) && ((reinterpret_cast<uintptr_t>(a) & 15) == 0);
         for (int rr = r0 + tid; rr < n; rr += BT) {
             float x[NB];
             float* row = a + (size_t)rr * lda + k0;
+            if (vec) {  // k0 is a multiple of NB: the row segment is 16-byte aligned
 #pragma unroll
-            for (int i = 0; i < NB; i++) x[i] = (i < kb) ? row[i] : 0.0f;
+                for (int i = 0; i < NB; i += 4) {
+                    const float4 v = *reinterpret_cast<const float4*>(row + i);
+                    x[i] = v.x, x[i + 1] = v.y, x[i + 2] = v.z, x[i + 3] = v.w;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < NB; i++) x[i] = row[i];
+            }
 #pragma unroll
             for (int k = 0; k < NB; k++)
 #pragma unroll
                 for (int i = k + 1; i < NB; i++) x[i] = fmaf(x[k], Ds[k * DL + i], x[i]);
+            if (vec) {
 #pragma unroll
-            for (int i = 0; i < NB; i++)
-                if (i < kb) row[i] = x[i];
+                for (int i = 0; i < NB; i += 4)
+                    *reinterpret_cast<float4*>(row + i) = make_float4(x[i], x[i + 1], x[i + 2], x[i + 3]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < NB; i++) row[i] = x[i];
+            }
         }
         __syncthreads();
-        // inner: C[r0:n, r0:n] += L * T
+        // inner: C[r0:n, r0:n] += L * T in 128 x 64 tiles, 8 x 4 per thread.  Per tile the
+        // C piece and the next top tile are in flight while the current tile's products run.
         const int ty = tid >> 4, tx = tid & 15;
-        const int tiles = (rem + TILE - 1) / TILE;
+        const int tiles_m = (rem + TM - 1) / TM, tiles_n = (rem + TN - 1) / TN;
         auto issue_top = [&](int tj, int buf) {
-            const int c0 = r0 + tj * TILE;
-            float* T = Tb + buf * (NB * TILE);
-            for (int idx = tid; idx < kb * TILE; idx += BT) {
-                const int k = idx / TILE, j = idx - k * TILE;
-                if (c0 + j < n)
-                    cp_async4(T + k * TILE + j, a + (size_t)(k0 + k) * lda + c0 + j);
-                else
-                    T[k * TILE + j] = 0.0f;
+            const int c0 = r0 + tj * TN;
+            float* T = Tb + buf * (NB * TN);
+            for (int idx = tid; idx < kb * TN / 4; idx += BT) {
+                const int k = idx / (TN / 4), j = (idx - k * (TN / 4)) * 4;
+                const float* src = a + (size_t)(k0 + k) * lda + c0 + j;
+                float* dst = T + k * TN + j;
+                if (vec && ((c0 + j) & 3) == 0 && c0 + j + 3 < n) {
+                    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        if (c0 + j + e < n)
+                            cp_async4(dst + e, src + e);
+                        else
+                            dst[e] = 0.0f;
+                    }
+                }
             }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
         };
-        const bool vec = ((lda & 3) == 0) && ((reinterpret_cast<uintptr_t>(a) & 15) == 0);
-        for (int ti = 0; ti < tiles; ti++) {
-            const int m0 = r0 + ti * TILE;
-            for (int idx = tid; idx < TILE * kb; idx += BT) {
+        for (int ti = 0; ti < tiles_m; ti++) {
+            const int m0 = r0 + ti * TM;
+            for (int idx = tid; idx < TM * kb; idx += BT) {
                 const int i = idx / kb, k = idx - i * kb;
                 if (m0 + i < n)
                     cp_async4(Lt + k * LS + i, a + (size_t)(m0 + i) * lda + k0 + k);
                 else
                     Lt[k * LS + i] = 0.0f;
             }
-            issue_top(0, 0);  // commits the left panel's copies with the first top tile
-            for (int tj = 0; tj < tiles; tj++) {
-                const int c0 = r0 + tj * TILE;
-                if (tj + 1 < tiles) issue_top(tj + 1, (tj + 1) & 1);
-                // this thread's 4 x 4 piece of C: loads in flight during the products
+            issue_top(0, 0);
+            asm volatile("cp.async.commit_group;\n" ::: "memory");  // left panel + first top tile
+            for (int tj = 0; tj < tiles_n; tj++) {
+                const int c0 = r0 + tj * TN;
+                if (tj + 1 < tiles_n) issue_top(tj + 1, (tj + 1) & 1);
+                asm volatile("cp.async.commit_group;\n" ::: "memory");  // the next top tile
+                // this thread's 8 x 4 piece of C, loaded now and consumed after the products
                 const int cc = c0 + tx * 4;
-                const bool full = vec && cc + 3 < n && ((cc & 3) == 0);
-                float cv[4][4];
+                const bool full = vec && cc + 3 < n;
+                float4 cv[8];
 #pragma unroll
-                for (int p = 0; p < 4; p++) {
-                    const int r = m0 + ty * 4 + p;
-                    if (r < n && full) {
-                        const float4 v = *reinterpret_cast<const float4*>(a + (size_t)r * lda + cc);
-                        cv[p][0] = v.x;
-                        cv[p][1] = v.y;
-                        cv[p][2] = v.z;
-                        cv[p][3] = v.w;
-                    } else {
-#pragma unroll
-                        for (int q = 0; q < 4; q++) cv[p][q] = (r < n && cc + q < n) ? a[(size_t)r * lda + cc + q] : 0.0f;
+                for (int p = 0; p < 8; p++) {
+                    const int r = m0 + ty * 8 + p;
+                    const float* src = a + (size_t)r * lda + cc;
+                    cv[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    if (r < n) {
+                        if (full) {
+                            cv[p] = __ldcg(reinterpret_cast<const float4*>(src));
+                        } else {
+                            if (cc < n) cv[p].x = src[0];
+                            if (cc + 1 < n) cv[p].y = src[1];
+                            if (cc + 2 < n) cv[p].z = src[2];
+                            if (cc + 3 < n) cv[p].w = src[3];
+                        }
                     }
                 }
-                if (tj + 1 < tiles)
-                    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-                else
-                    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+                asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this top tile (earlier group)
                 __syncthreads();
-                const float* T = Tb + (tj & 1) * (NB * TILE);
-                float acc[4][4];
+                const float* T = Tb + (tj & 1) * (NB * TN);
+                float acc[8][4];
 #pragma unroll
-                for (int p = 0; p < 4; p++)
+                for (int p = 0; p < 8; p++)
 #pragma unroll
                     for (int q = 0; q < 4; q++) acc[p][q] = 0.0f;
-#pragma unroll 8
-                for (int k = 0; k < kb; k++) {
-                    const float4 lv = *reinterpret_cast<const float4*>(Lt + k * LS + ty * 4);
-                    const float4 tv = *reinterpret_cast<const float4*>(T + k * TILE + tx * 4);
-                    const float l4[4] = {lv.x, lv.y, lv.z, lv.w};
+#pragma unroll
+                for (int k = 0; k < NB; k++) {  // kb == NB here
+                    const float4 l0 = *reinterpret_cast<const float4*>(Lt + k * LS + ty * 8);
+                    const float4 l1 = *reinterpret_cast<const float4*>(Lt + k * LS + ty * 8 + 4);
+                    const float4 tv = *reinterpret_cast<const float4*>(T + k * TN + tx * 4);
+                    const float l8[8] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
                     const float t4[4] = {tv.x, tv.y, tv.z, tv.w};
 #pragma unroll
-                    for (int p = 0; p < 4; p++)
+                    for (int p = 0; p < 8; p++)
 #pragma unroll
-                        for (int q = 0; q < 4; q++) acc[p][q] = fmaf(l4[p], t4[q], acc[p][q]);
+                        for (int q = 0; q < 4; q++) acc[p][q] = fmaf(l8[p], t4[q], acc[p][q]);
                 }
 #pragma unroll
-                for (int p = 0; p < 4; p++) {
-                    const int r = m0 + ty * 4 + p;
+                for (int p = 0; p < 8; p++) {
+                    const int r = m0 + ty * 8 + p;
                     if (r >= n) continue;
+                    float* dst = a + (size_t)r * lda + cc;
                     if (full) {
-                        *reinterpret_cast<float4*>(a + (size_t)r * lda + cc) =
-                            make_float4(cv[p][0] + acc[p][0], cv[p][1] + acc[p][1], cv[p][2] + acc[p][2],
-                                        cv[p][3] + acc[p][3]);
+                        *reinterpret_cast<float4*>(dst) = make_float4(cv[p].x + acc[p][0], cv[p].y + acc[p][1],
+                                                                      cv[p].z + acc[p][2], cv[p].w + acc[p][3]);
                     } else {
-#pragma unroll
-                        for (int q = 0; q < 4; q++)
-                            if (cc + q < n) a[(size_t)r * lda + cc + q] = cv[p][q] + acc[p][q];
+                        if (cc < n) dst[0] = cv[p].x + acc[p][0];
+                        if (cc + 1 < n) dst[1] = cv[p].y + acc[p][1];
+                        if (cc + 2 < n) dst[2] = cv[p].z + acc[p][2];
+                        if (cc + 3 < n) dst[3] = cv[p].w + acc[p][3];
                     }
                 }
-                __syncthreads();  // this buffer is refilled two tiles later; Lt stays until the row block ends
+                __syncthreads();  // this top buffer is refilled next; Lt stays for the row block
             }
         }
     }
 }
 
-// Blocked forward/back sweeps, right-hand sides resident in shared memory.
+// Blocked forward/back sweeps, right-hand sides resident in shared memory
+// (nrhs <= NR).  Per 64-unknown block: the diagonal block is staged in shared
+// memory and one warp per right-hand side walks its 64-step chain (values in
+// lanes, pivots by shuffle); then every thread updates up to four later
+// (forward) / earlier (backward) unknowns with the block's rows, loading each
+// factor element once for all right-hand sides.
+constexpr int kSolveBlk = 64;
+__shared__ float s_dblk[kSolveBlk * (kSolveBlk + 1)];  // one diagonal block, shared by every instantiation
+
+template <int NR>
 __device__ __noinline__ void solve_blocked(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* sm) {
-    constexpr int SBK = 64, DL = SBK + 1;
-    float* Y = sm;                       // nrhs x n
+    constexpr int SBK = kSolveBlk, DL = SBK + 1, PT = 4;  // unknowns per thread in the update
+    float* Y = sm;                                        // nrhs x n
+    float* Dblk = s_dblk;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    __shared__ float Dblk[SBK * DL];
-    __shared__ float scq[RHS_MAX];
     for (int idx = tid; idx < nrhs * n; idx += BT) {
         const int q = idx / n, i = idx - q * n;
         Y[idx] = b[(size_t)q * ldb + i];
@@ -349,19 +383,33 @@ __device__ __noinline__ void solve_blocked(const float* a, int lda, int n, float
             if (lane + 32 < kb) y[lane + 32] = v1;
         }
         __syncthreads();
-        for (int i = k0 + kb + tid; i < n; i += BT) {
-            float acc[RHS_MAX];
+        for (int i0 = k0 + kb + tid; i0 < n; i0 += PT * BT) {
+            float acc[PT][NR];
 #pragma unroll
-            for (int q = 0; q < RHS_MAX; q++) acc[q] = 0.0f;
+            for (int e = 0; e < PT; e++)
+#pragma unroll
+                for (int q = 0; q < NR; q++) acc[e][q] = 0.0f;
             for (int k = 0; k < kb; k++) {
-                const float s = a[(size_t)(k0 + k) * lda + i];
+                const float* row = a + (size_t)(k0 + k) * lda;
+                float yk[NR];
 #pragma unroll
-                for (int q = 0; q < RHS_MAX; q++)
-                    if (q < nrhs) acc[q] = fmaf(Y[q * n + k0 + k], s, acc[q]);
+                for (int q = 0; q < NR; q++) yk[q] = q < nrhs ? Y[q * n + k0 + k] : 0.0f;
+#pragma unroll
+                for (int e = 0; e < PT; e++) {
+                    const int i = i0 + e * BT;
+                    const float s = i < n ? row[i] : 0.0f;
+#pragma unroll
+                    for (int q = 0; q < NR; q++) acc[e][q] = fmaf(yk[q], s, acc[e][q]);
+                }
             }
 #pragma unroll
-            for (int q = 0; q < RHS_MAX; q++)
-                if (q < nrhs) Y[q * n + i] += acc[q];
+            for (int e = 0; e < PT; e++) {
+                const int i = i0 + e * BT;
+                if (i < n)
+#pragma unroll
+                    for (int q = 0; q < NR; q++)
+                        if (q < nrhs) Y[q * n + i] += acc[e][q];
+            }
         }
         __syncthreads();
     }
@@ -378,31 +426,45 @@ __device__ __noinline__ void solve_blocked(const float* a, int lda, int n, float
             float v0 = lane < kb ? y[lane] : 0.0f, v1 = lane + 32 < kb ? y[lane + 32] : 0.0f;
             for (int k = kb - 1; k >= 0; k--) {
                 const float yk = __shfl_sync(0xffffffffu, k < 32 ? v0 : v1, k & 31);
-                const float s = yk * Dblk[k * DL + k];
+                const float sk = yk * Dblk[k * DL + k];
                 if (lane == (k & 31)) {
-                    if (k < 32) v0 = -s; else v1 = -s;
+                    if (k < 32) v0 = -sk; else v1 = -sk;
                 }
-                if (lane < k) v0 = fmaf(s, Dblk[k * DL + lane], v0);
-                if (lane + 32 < k) v1 = fmaf(s, Dblk[k * DL + lane + 32], v1);
+                if (lane < k) v0 = fmaf(sk, Dblk[k * DL + lane], v0);
+                if (lane + 32 < k) v1 = fmaf(sk, Dblk[k * DL + lane + 32], v1);
             }
             if (lane < kb) y[lane] = v0;
             if (lane + 32 < kb) y[lane + 32] = v1;
         }
         __syncthreads();
         // coefficients s_k = -x_k of this block update the unknowns before it
-        for (int i = tid; i < k0; i += BT) {
-            float acc[RHS_MAX];
+        for (int i0 = tid; i0 < k0; i0 += PT * BT) {
+            float acc[PT][NR];
 #pragma unroll
-            for (int q = 0; q < RHS_MAX; q++) acc[q] = 0.0f;
+            for (int e = 0; e < PT; e++)
+#pragma unroll
+                for (int q = 0; q < NR; q++) acc[e][q] = 0.0f;
             for (int k = 0; k < kb; k++) {
-                const float s = a[(size_t)(k0 + k) * lda + i];
+                const float* row = a + (size_t)(k0 + k) * lda;
+                float sk[NR];
 #pragma unroll
-                for (int q = 0; q < RHS_MAX; q++)
-                    if (q < nrhs) acc[q] = fmaf(-Y[q * n + k0 + k], s, acc[q]);
+                for (int q = 0; q < NR; q++) sk[q] = q < nrhs ? -Y[q * n + k0 + k] : 0.0f;
+#pragma unroll
+                for (int e = 0; e < PT; e++) {
+                    const int i = i0 + e * BT;
+                    const float s = i < k0 ? row[i] : 0.0f;
+#pragma unroll
+                    for (int q = 0; q < NR; q++) acc[e][q] = fmaf(sk[q], s, acc[e][q]);
+                }
             }
 #pragma unroll
-            for (int q = 0; q < RHS_MAX; q++)
-                if (q < nrhs) Y[q * n + i] += acc[q];
+            for (int e = 0; e < PT; e++) {
+                const int i = i0 + e * BT;
+                if (i < k0)
+#pragma unroll
+                    for (int q = 0; q < NR; q++)
+                        if (q < nrhs) Y[q * n + i] += acc[e][q];
+            }
         }
         __syncthreads();
     }
@@ -437,7 +499,12 @@ __global__ void __launch_bounds__(BT, 2) k_batch_solve(const BatchSys* __restric
                 else
                     factor_blocked<32>(a, s.lda, s.n, sm);
             }
-            solve_blocked(a, s.lda, s.n, b, s.ldb, nrhs, sm);
+            if (nrhs == 1)
+                solve_blocked<1>(a, s.lda, s.n, b, s.ldb, nrhs, sm);
+            else if (nrhs <= 4)
+                solve_blocked<4>(a, s.lda, s.n, b, s.ldb, nrhs, sm);
+            else
+                solve_blocked<16>(a, s.lda, s.n, b, s.ldb, nrhs, sm);
         }
     }
 }
