@@ -47,6 +47,18 @@ constexpr int kBatchSolveOnly = 1 << 8;
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
                 int max_iters, int* iters, double* resid, cudaStream_t st);
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
+// Partial pivoting (k_pivot.cu): kernels of the blocked LINPACK-convention LU.
+int piv_init_attrs();
+size_t piv_sync_bytes();
+int piv_panel_width(int n, int sms);
+int launch_piv_panel(float* a, int lda, int n, int k0, int kb, int* ipvt, unsigned char* sync, unsigned* bar_base,
+                     int sms, cudaStream_t st);
+int launch_piv_rows(float* a, int lda, int n, int k0, int pb, const int* ipvt, float* at, int ldat, int sms,
+                    cudaStream_t st);
+int launch_piv_desc(const int* ipvt, int n, int pb, int* desc, cudaStream_t st);
+int launch_piv_convert(float* a, int lda, int n, int pb, const int* ipvt, bool to_reference, cudaStream_t st);
+int launch_piv_gesl(const float* a, int lda, int n, int pb, const int* desc, float* b, int ldb, int nrhs, float* w,
+                    unsigned char* sync, int sms, cudaStream_t st);
 // Waits for the work queued on st so far without spinning a CPU core.
 int wait_stream(lp_ctx* c, cudaStream_t st);
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
@@ -83,6 +95,8 @@ struct lp_ctx {
     lp::Workspace dnorm;                      // refinement norms (device)
     unsigned long long* hnorm = nullptr;      // their pinned host copy
     size_t hnorm_cap = 0;
+    lp::Workspace psync, pat, pdesc, pw, pipvt;  // pivoting: barrier + exchange area, transposed U12,
+                                                 // interchange permutations, solve vectors, ipvt
     lp::Workspace bsys, bnext;                // batched: sorted system descriptors, work counter
     lp::Workspace tA, tB;                     // batched autotuner: scratch copies of the inputs
     uint64_t bsys_hash = 0;                   // descriptors + configuration of the cached graph
@@ -100,7 +114,7 @@ struct lp_ctx {
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
         lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
-                                &dnorm, &bsys, &bnext, &tA, &tB};
+                                &dnorm, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
         bgraph = nullptr;

@@ -30,6 +30,7 @@ PRECISIONS = {"f32": LP_F32, "bf16": LP_BF16_IR, "fp8": LP_FP8_IR}
 
 _F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_I32P = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _VP = ctypes.c_void_p
 _I = ctypes.c_int
 
@@ -168,6 +169,9 @@ def lib() -> ctypes.CDLL:
     L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
     L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
+    L.lp_gefa_pvt_dev.argtypes = [_VP, _VP, _I, _I, _VP]
+    L.lp_gesl_pvt_dev.argtypes = [_VP, _VP, _I, _I, _VP, _VP, _I, _I]
+    L.lp_calculate_pvt.argtypes = [_VP, _I, _I, _I, _F32P, _F32P, _I32P, _F64P, _F64P]
     L.lp_solve_host.argtypes = [_VP, _I, _I, _I, _F32P, _I, _F64P, _I, _F64P, _I, ctypes.POINTER(LpTiming)]
     L.lp_batch_default_config.argtypes = [ctypes.POINTER(LpBatchConfig)]
     L.lp_batch_solve_dev.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig),
@@ -329,6 +333,26 @@ class Context:
 
     def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
         check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")
+
+    # ---- partial pivoting (gefa_ref / gesl_ref) -------------------------------
+    def gefa_pvt(self, dA: int, n: int, lda: int, dIpvt: int) -> None:
+        """LU with partial pivoting in place (reference encoding); dIpvt: n ints."""
+        check(lib().lp_gefa_pvt_dev(self._h, dA, n, lda, dIpvt), "lp_gefa_pvt_dev")
+
+    def gesl_pvt(self, dLU: int, n: int, lda: int, dIpvt: int, dB: int, nrhs: int = 1,
+                 ldb: int | None = None) -> None:
+        check(lib().lp_gesl_pvt_dev(self._h, dLU, n, lda, dIpvt, dB, nrhs, n if ldb is None else ldb),
+              "lp_gesl_pvt_dev")
+
+    def calculate_pvt(self, A: np.ndarray, b: np.ndarray, repetitions: int = 1):
+        """The backend for non-diagonally-dominant matrices: A -> factors
+        (gefa_ref encoding), b -> x.  Returns ({"gefa": [...], "gesl": [...]}, ipvt)."""
+        n = A.shape[0]
+        tg = np.zeros(repetitions, np.float64)
+        ts = np.zeros(repetitions, np.float64)
+        ipvt = np.zeros(n, np.int32)
+        check(lib().lp_calculate_pvt(self._h, n, A.shape[1], repetitions, A, b, ipvt, tg, ts), "lp_calculate_pvt")
+        return {"gefa": tg.tolist(), "gesl": ts.tolist()}, ipvt
 
     # ---- batched solves ---------------------------------------------------
     def batch_solve(self, systems, dA: int, dB: int, cfg: "LpBatchConfig | None" = None) -> dict:

@@ -195,6 +195,23 @@ int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nr
  * lp_gesl_dev; the solutions overwrite dB. */
 int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, void* stream);
 
+/* ---- LU with partial pivoting (device pointers) ------------------------------
+ * The reference's gefa_ref / gesl_ref (LINPACK/src/host/linpack_data.cpp:72-156),
+ * which its harness uses for matrices that are not diagonally dominant
+ * (the --uniform option, linpack_benchmark.hpp:69, 440-447).  LINPACK
+ * convention: ipvt[k] is the row exchanged with row k at step k (the first
+ * largest magnitude); the exchange of step k touches only the columns >= k
+ * of M = S^T; on return the diagonal holds u_kk, the rest of each storage
+ * row right of it the negated multipliers, left of it U — the bytes
+ * gefa_ref leaves (up to rounding: the trailing updates are blocked).
+ * For n > 128, n and lda must be multiples of 4 and dA 16-byte aligned. */
+int lp_gefa_pvt_dev(lp_ctx* ctx, float* dA, int n, int lda, int* dIpvt);
+/* Forward (with the interchanges) and back substitution with such factors,
+ * nrhs right-hand sides as rows of dB (overwritten by the solutions).  The
+ * factors are permuted in place during the call and restored exactly before
+ * it returns. */
+int lp_gesl_pvt_dev(lp_ctx* ctx, float* dLU, int n, int lda, const int* dIpvt, float* dB, int nrhs, int ldb);
+
 /* ---- host entry points --------------------------------------------------- */
 /* The CUDA execution backend: the drop-in for
  *   std::map<std::string, std::vector<double>> execution::pcie::calculate(
@@ -208,6 +225,13 @@ int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, i
  * linpack_benchmark.hpp:321-323), b holds the solution x. */
 int lp_calculate(lp_ctx* ctx, int n, int lda, int bs, int repetitions, float* A, float* b,
                  double* gefa_times, double* gesl_times);
+/* The same backend for matrices that are not diagonally dominant (the
+ * harness's --uniform case): partial pivoting, LINPACK convention.  On return
+ * A holds the factors in gefa_ref's encoding, ipvt (n entries) the pivots,
+ * b the solution x.  gefa_times include putting the factors into that
+ * encoding; gesl_times the forward (with interchanges) and back substitution. */
+int lp_calculate_pvt(lp_ctx* ctx, int n, int lda, int repetitions, float* A, float* b, int* ipvt,
+                     double* gefa_times, double* gesl_times);
 
 /* Factor a host matrix in place and solve for host right-hand sides, with
  * the chosen precision; copies are part of the call and are timed in t.

@@ -64,6 +64,10 @@ def orc():
         lib.orc_gefa_nopvt_f64.argtypes = [_F64P, c_int, c_int]
         lib.orc_gesl_nopvt_f32.argtypes = [_F32P, _F32P, c_int, c_int]
         lib.orc_gesl_nopvt_f64.argtypes = [_F64P, _F64P, c_int, c_int]
+        lib.orc_gefa_pvt_f32.argtypes = [_F32P, c_int, c_int, _I32P]
+        lib.orc_gefa_pvt_f64.argtypes = [_F64P, c_int, c_int, _I32P]
+        lib.orc_gesl_pvt_f32.argtypes = [_F32P, _F32P, _I32P, c_int, c_int]
+        lib.orc_gesl_pvt_f64.argtypes = [_F64P, _F64P, _I32P, c_int, c_int]
         lib.orc_top_update_f32.argtypes = [_F32P, c_int, _F32P, c_int, c_int, c_int]
         lib.orc_left_update_f32.argtypes = [_F32P, c_int, _F32P, c_int, c_int, c_int]
         lib.orc_inner_update_f32.argtypes = [_F32P, c_int, _F32P, c_int, _F32P, c_int, c_int, c_int, c_int]
@@ -100,6 +104,8 @@ def ref(precision: str = "f32"):
         if lib is not None:
             lib.ref_gefa_nopvt_f64.argtypes = [_F64P, ctypes.c_uint, ctypes.c_uint]
             lib.ref_gesl_nopvt_f64.argtypes = [_F64P, _F64P, ctypes.c_uint, ctypes.c_uint]
+            lib.ref_gefa_pvt_f64.argtypes = [_F64P, ctypes.c_uint, ctypes.c_uint, _I32P]
+            lib.ref_gesl_pvt_f64.argtypes = [_F64P, _F64P, _I32P, ctypes.c_uint, ctypes.c_uint]
         _ref64 = lib
     return _ref64
 
@@ -146,6 +152,33 @@ def gesl_nopvt(LU: np.ndarray, b: np.ndarray) -> np.ndarray:
     else:
         x = np.ascontiguousarray(b, dtype=np.float64).copy()
         orc().orc_gesl_nopvt_f64(lu, x, n, lu.shape[1])
+    return x
+
+
+def gefa_pvt(A: np.ndarray):
+    """Unblocked LU with partial pivoting (LINPACK convention, reference
+    encoding): returns (factors, ipvt) as copies."""
+    a = np.ascontiguousarray(A).copy()
+    n = a.shape[0]
+    ipvt = np.zeros(max(n, 1), dtype=np.int32)
+    if a.dtype == np.float32:
+        orc().orc_gefa_pvt_f32(a, n, a.shape[1], ipvt)
+    else:
+        a = a.astype(np.float64)
+        orc().orc_gefa_pvt_f64(a, n, a.shape[1], ipvt)
+    return a, ipvt[:n]
+
+
+def gesl_pvt(LU: np.ndarray, ipvt: np.ndarray, b: np.ndarray) -> np.ndarray:
+    lu = np.ascontiguousarray(LU)
+    n = lu.shape[0]
+    piv = np.ascontiguousarray(ipvt, dtype=np.int32)
+    if lu.dtype == np.float32:
+        x = np.ascontiguousarray(b, dtype=np.float32).copy()
+        orc().orc_gesl_pvt_f32(lu, x, piv, n, lu.shape[1])
+    else:
+        x = np.ascontiguousarray(b, dtype=np.float64).copy()
+        orc().orc_gesl_pvt_f64(lu, x, piv, n, lu.shape[1])
     return x
 
 

@@ -62,6 +62,65 @@ void orc_gefa_nopvt_f64(double* a, int n, int lda) { GEFA_BODY(double) }
 void orc_gesl_nopvt_f32(const float* a, float* b, int n, int lda) { GESL_BODY(float) }
 void orc_gesl_nopvt_f64(const double* a, double* b, int n, int lda) { GESL_BODY(double) }
 
+/* LINPACK/src/host/linpack_data.cpp:72-117 (gefa_ref, partial pivoting,
+ * LINPACK dgefa convention).  Step k (k < n-1): the pivot is the first
+ * largest |S[k][i]|, i >= k (M's column k, a strict "<" scan, so the first
+ * of equal magnitudes wins and a NaN never displaces the running maximum);
+ * storage rows i >= k exchange entries k and p (M's rows k and p, columns
+ * >= k only: earlier multipliers stay where they were computed); storage
+ * row k's entries i > k are scaled by -1/d (the reciprocal taken in double,
+ * the product rounded to T); every storage row j > k receives
+ * S[j][i] += S[k][i] * S[j][k] for i > k.  The diagonal keeps d. */
+#define GEFA_PVT_BODY(T)                                                    \
+    for (int i = 0; i < n; i++) ipvt[i] = i;                                \
+    for (int k = 0; k + 1 < n; k++) {                                       \
+        T* rowk = a + (size_t)k * lda;                                      \
+        int p = k;                                                          \
+        T best = (T)fabs((double)rowk[k]);                                  \
+        for (int i = k + 1; i < n; i++) {                                   \
+            const T v = (T)fabs((double)rowk[i]);                           \
+            if (best < v) { best = v; p = i; }                              \
+        }                                                                   \
+        for (int j = k; j < n; j++) {                                       \
+            T* rowj = a + (size_t)j * lda;                                  \
+            const T t = rowj[k]; rowj[k] = rowj[p]; rowj[p] = t;            \
+        }                                                                   \
+        ipvt[k] = p;                                                        \
+        const double s = -1.0 / (double)rowk[k];                            \
+        for (int i = k + 1; i < n; i++) rowk[i] = (T)((double)rowk[i] * s); \
+        for (int j = k + 1; j < n; j++) {                                   \
+            T* rowj = a + (size_t)j * lda;                                  \
+            const T f = rowj[k];                                            \
+            for (int i = k + 1; i < n; i++) rowj[i] += rowk[i] * f;         \
+        }                                                                   \
+    }
+
+void orc_gefa_pvt_f32(float* a, int n, int lda, int* ipvt) { GEFA_PVT_BODY(float) }
+void orc_gefa_pvt_f64(double* a, int n, int lda, int* ipvt) { GEFA_PVT_BODY(double) }
+
+/* LINPACK/src/host/linpack_data.cpp:119-156 (gesl_ref).  Forward: for
+ * k < n-1, exchange y[k] and y[ipvt[k]], then y[i] += y[k] * S[k][i] (i > k).
+ * Backward: y[k] /= S[k][k]; y[i] -= y[k] * S[k][i] (i < k). */
+#define GESL_PVT_BODY(T)                                                    \
+    T* y = (T*)malloc(sizeof(T) * (size_t)(n > 0 ? n : 1));                 \
+    for (int k = 0; k < n; k++) y[k] = b[k];                                \
+    for (int k = 0; k + 1 < n; k++) {                                       \
+        const int p = ipvt[k];                                              \
+        if (p != k) { const T t = y[k]; y[k] = y[p]; y[p] = t; }            \
+        const T* rowk = a + (size_t)k * lda;                                \
+        for (int i = k + 1; i < n; i++) y[i] += y[k] * rowk[i];             \
+    }                                                                       \
+    for (int k = n - 1; k >= 0; k--) {                                      \
+        const T* rowk = a + (size_t)k * lda;                                \
+        y[k] = y[k] / rowk[k];                                              \
+        for (int i = 0; i < k; i++) y[i] -= y[k] * rowk[i];                 \
+    }                                                                       \
+    for (int k = 0; k < n; k++) b[k] = y[k];                                \
+    free(y);
+
+void orc_gesl_pvt_f32(const float* a, float* b, const int* ipvt, int n, int lda) { GESL_PVT_BODY(float) }
+void orc_gesl_pvt_f64(const double* a, double* b, const int* ipvt, int n, int lda) { GESL_PVT_BODY(double) }
+
 /* Same solve for nrhs right-hand sides stored as rows: B[r*ldb + i]. */
 void orc_gesl_nopvt_multi_f64(const double* a, double* B, int n, int lda, int nrhs, int ldb) {
     for (int r = 0; r < nrhs; r++) orc_gesl_nopvt_f64(a, B + (size_t)r * ldb, n, lda);

@@ -156,3 +156,73 @@ def test_hpl_residual_definition():
     want = np.abs(r).max() / (np.abs(M).sum(axis=1).max() * np.abs(x).max() + np.abs(b64).max()) / n / (oracle.DBL_EPS / 2)
     assert np.isclose(oracle.hpl_resid(A, x, b64), want, rtol=1e-6)  # r is a cancelling difference
     assert np.allclose(oracle.residual_f64(A, x, b64), r, rtol=0, atol=1e-9)
+
+
+# ---- partial pivoting: gefa_ref / gesl_ref (linpack_data.cpp:72-156) ------------
+
+def _pivot_cases(n, rng):
+    """A uniform (non-dominant) matrix plus edge cases of the pivot search:
+    a zero diagonal, equal magnitudes of opposite sign (the first wins)."""
+    A = rng.random((n, n)).astype(np.float32)
+    if n >= 4:
+        A[0, 0] = 0.0                       # step 0 must exchange
+        A[1, 1:] = 0.5
+        A[1, 3] = -0.5                      # |.| tie in M's column 1
+        A[1, 1] = 0.25
+    return A
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 33, 128, 257])
+def test_pivot_restatement_bitexact_vs_reference_f32(n):
+    ref = need_ref("f32")
+    A = _pivot_cases(n, np.random.default_rng(n))
+    mine, p_mine = oracle.gefa_pvt(A)
+    theirs = A.copy()
+    p_ref = np.zeros(n, np.int32)
+    ref.ref_gefa_pvt_f32(theirs, n, n, p_ref)
+    assert np.array_equal(p_mine, p_ref)
+    assert np.array_equal(bits(mine), bits(theirs))
+    b = np.random.default_rng(1).random(n).astype(np.float32)
+    x_mine = oracle.gesl_pvt(mine, p_mine, b)
+    x_ref = b.copy()
+    ref.ref_gesl_pvt_f32(theirs, x_ref, p_ref, n, n)
+    assert np.array_equal(bits(x_mine), bits(x_ref))
+
+
+@pytest.mark.parametrize("n", [16, 100])
+def test_pivot_restatement_bitexact_vs_reference_f64(n):
+    ref = need_ref("f64")
+    A = _pivot_cases(n, np.random.default_rng(7)).astype(np.float64)
+    mine, p_mine = oracle.gefa_pvt(A)
+    theirs = A.copy()
+    p_ref = np.zeros(n, np.int32)
+    ref.ref_gefa_pvt_f64(theirs, n, n, p_ref)
+    assert np.array_equal(p_mine, p_ref)
+    assert np.array_equal(bits(mine), bits(theirs))
+
+
+def test_pivot_search_semantics():
+    """First of equal magnitudes; NaN below the diagonal never chosen; a NaN
+    diagonal is kept (the reference's strict '<' scan)."""
+    S = np.eye(4, dtype=np.float32)
+    S[0] = [0.5, -2.0, 2.0, 1.0]            # M's column 0: tie between rows 1 and 2
+    _, p = oracle.gefa_pvt(S)
+    assert p[0] == 1
+    S = np.eye(4, dtype=np.float32) * 3
+    S[0] = [1.0, np.nan, 2.0, 0.0]
+    _, p = oracle.gefa_pvt(S)
+    assert p[0] == 2
+    S[0] = [np.nan, 5.0, 2.0, 0.0]
+    _, p = oracle.gefa_pvt(S)
+    assert p[0] == 0
+
+
+def test_pivot_solution_uniform_reference_input():
+    """The harness's --uniform input (no diagonal dominance) solves to
+    x = ones with the reference's residn < 1."""
+    n = 200
+    A, b, _, normb = oracle.gen_reference(n, diag_dominant=False)
+    lu, p = oracle.gefa_pvt(A)
+    x = oracle.gesl_pvt(lu, p, b)
+    rn, _ = oracle.residn(x, normb)
+    assert rn < 1.0
