@@ -249,6 +249,71 @@ def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
 FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
 
 
+def run_pivot(ctx, lp, torch, stream, n, steps, warmup, pk) -> dict:
+    """LU with partial pivoting (the harness's --uniform case, gefa_ref /
+    gesl_ref convention) on a non-dominant matrix: U(0,1) entries (seed 42,
+    torch's device generator), b = column sums of the storage (x = ones).
+    A step = restore A, lp_gefa_pvt_dev + lp_gesl_pvt_dev, on device time."""
+    with torch.cuda.stream(stream):
+        g = torch.Generator(device="cuda")
+        g.manual_seed(42)
+        dA0 = torch.rand((n, n), generator=g, device="cuda", dtype=torch.float32)
+        db0 = torch.zeros(n, dtype=torch.float64, device="cuda")
+        for r in range(0, n, 4096):
+            db0 += dA0[r:r + 4096].double().sum(0)
+        db0 = db0.float()
+        dA = torch.empty_like(dA0)
+        dB = torch.empty_like(db0)
+        dP = torch.zeros(n, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+            dB.copy_(db0)
+        ctx.gefa_pvt(dA.data_ptr(), n, n, dP.data_ptr())
+        ctx.gesl_pvt(dA.data_ptr(), n, n, dP.data_ptr(), dB.data_ptr(), 1, n)
+
+    for _ in range(warmup):
+        step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.read_profile(reset=True)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    prof = ctx.read_profile(reset=True)
+    ctx.set_profiling(False)
+    x = dB.double()
+    resid = float((x - 1.0).abs().max())
+    normb = float(db0.max())
+    swaps = int((dP.cpu().numpy() != np.arange(n)).sum())
+    inner = prof["inner"]
+    tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
+    stage_s = {k: prof[k]["s"] for k in lp.STAGES if prof[k]["calls"]}
+    tot = sum(stage_s.values())
+    return {
+        "workload": f"FP32 LU with partial pivoting + substitution, n={n}, U(0,1) entries (no diagonal dominance), "
+                    "b = A*ones, seed 42",
+        "value": steps * flops(n) / t / 1e9, "unit": UNIT, "ms_per_step": 1e3 * t / steps,
+        "row_exchanges": swaps, "max_abs_err_x": resid,
+        "residn": resid / (n * normb * float(np.finfo(np.float32).eps)),
+        "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)", "achieved": tfs,
+                     "unit": "TFLOP/s"},
+        "stages": {k: {"s": v, "share": v / tot if tot > 0 else None, "calls": prof[k]["calls"]}
+                   for k, v in stage_s.items()},
+        "stage_names": {"lu": "k_piv_panel (pivot search, exchange, panel update)",
+                        "left": "k_piv_rows (interchanges + triangular solve of the block row)",
+                        "inner": "k_sgemm_update", "gesl": "k_piv_gesl"},
+    }
+
+
 RESERVE = 110 * 10 ** 9  # pool mapped at start: the 80 GB budget plus headroom against fragmentation
 
 
@@ -331,6 +396,7 @@ def main() -> None:
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-pivot", action="store_true")
     ap.add_argument("--serve-rates", default="100,200,300,400,500,600,700,800,900,1000,1250,1500,2000,5000,20000")
     ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
@@ -425,6 +491,13 @@ def main() -> None:
             mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, args.steps,
                                     max(1, min(args.warmup, 2)), value / world, pk)
 
+    pivot = None
+    if not args.no_pivot:
+        pivot = run_pivot(ctx, lp, torch, stream, n, args.steps, max(1, min(args.warmup, 2)), pk)
+        if pivot is not None and pivot["roofline"]["achieved"]:
+            pivot["roofline"]["peak"] = peak_tf
+            pivot["roofline"]["frac"] = pivot["roofline"]["achieved"] / peak_tf
+
     batched = None
     if not args.no_batch:
         batched = run_batched(ctx, lp, torch, stream, args.steps, max(1, min(args.warmup, 2)), args.batch_count)
@@ -488,7 +561,12 @@ def main() -> None:
                      "peak_source": f"derived: {NUM_SMS} SMs x {FP32_LANES_PER_SM} FP32 lanes x 2 flop x median SM "
                                     f"clock under load ({sm_mhz} MHz); MEASURED_PEAKS.json has no FP32 figure",
                      "per_unit": "2*m*m*bs flop per trailing update of an m x m trailing matrix",
-                     "launches": inner["calls"], "traffic": None},
+                     "launches": inner["calls"],
+                     # DRAM bytes per trailing update: the n=8192 ncu capture of this kernel
+                     # (profiles/k_sgemm_update_n8192_b512.md) read+wrote 452.4 MB for 503.3 MB of
+                     # algorithmic bytes; scaled by the algorithmic bytes of this run's updates.
+                     "traffic": (inner["bytes"] / inner["calls"] * 452.4 / 503.3) if inner["calls"] else None,
+                     "traffic_unit": "bytes per trailing update (scaled from the n=8192 capture)"},
         "stages": {k: {"s": prof[k]["s"], "share": stage_share[k], "calls": prof[k]["calls"]} for k in lp.STAGES
                    if prof[k]["calls"]},
         "gesl": {"s_per_step": gesl["s"] / max(1, args.steps),
@@ -499,6 +577,8 @@ def main() -> None:
     }
     if mixed:
         line["mixed"] = mixed
+    if pivot is not None:
+        line["pivot"] = pivot
     if batched is not None:
         line["batched"] = batched
     if serving is not None:

@@ -138,6 +138,19 @@ inline std::map<std::string, std::vector<double>> calculate(
     return {{"gefa", gefa}, {"gesl", gesl}};
 }
 
+// Matrices without diagonal dominance (--uniform): partial pivoting with
+// the reference's gefa_ref / gesl_ref convention (linpack_data.cpp:72-156);
+// data.ipvt receives the pivots.
+inline std::map<std::string, std::vector<double>> calculate_pvt(
+    const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data) {
+    const auto& s = *config.programSettings;
+    std::vector<double> gefa(s.numRepetitions), gesl(s.numRepetitions);
+    check_lp(lp_calculate_pvt(config.context, (int)s.matrixSize, (int)data.matrix_width, (int)s.numRepetitions, data.A,
+                              data.b, data.ipvt, gefa.data(), gesl.data()),
+             "lp_calculate_pvt");
+    return {{"gefa", gefa}, {"gesl", gesl}};
+}
+
 // Mixed precision (addition): tensor-core trailing updates, FP64 refinement.
 inline std::map<std::string, std::vector<double>> calculate_mixed(
     const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data, int* iters,
@@ -216,12 +229,14 @@ public:
     // linpack_benchmark.hpp:306-324
     void executeKernel(LinpackData& data) override {
         const auto& s = *executionSettings->programSettings;
-        if (!s.isDiagonallyDominant)
-            throw std::runtime_error("Uniform (non diagonally dominant) matrices need pivoting, which the CUDA kernels "
-                                     "do not implement");
+        if (!s.isDiagonallyDominant && s.precision != "f32")
+            throw std::runtime_error("Uniform (non diagonally dominant) matrices are solved with partial pivoting in "
+                                     "FP32 only (--precision f32)");
         switch (s.communicationType) {
             case CommunicationType::cuda:
-                if (s.precision == "f32")
+                if (!s.isDiagonallyDominant)
+                    this->timings = execution::cuda::calculate_pvt(*executionSettings, data);
+                else if (s.precision == "f32")
                     this->timings = execution::cuda::calculate(*executionSettings, data);
                 else
                     this->timings = execution::cuda::calculate_mixed(*executionSettings, data, &ir_iterations_,

@@ -113,7 +113,21 @@ def test_lp_bench_unsupported_comm_type(lp):
 
 
 @pytest.mark.gpu
-def test_lp_bench_uniform_matrix_rejected(lp):
-    r = run(["-f", "hpl_CUDA", "-m", "2", "-b", "5", "--uniform"])
+@pytest.mark.parametrize("m,b", [(2, 5), (8, 7)])
+def test_lp_bench_uniform_matrix_pivoting(tmp_path, lp, m, b):
+    """--uniform: no diagonal dominance, solved with partial pivoting
+    (gefa_ref / gesl_ref convention) and validated as the reference does."""
+    out = tmp_path / "uniform.json"
+    r = run(["-f", "hpl_CUDA", "-m", str(m), "-b", str(b), "-n", "2", "--uniform", "--dump-json", str(out)])
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Validation: SUCCESS!" in r.stdout
+    j = json.loads(out.read_text())
+    assert j["settings"]["Diagonally Dominant"] in (False, "No")
+    assert j["errors"]["residual_norm"] < 1.0
+
+
+@pytest.mark.gpu
+def test_lp_bench_uniform_mixed_rejected(lp):
+    r = run(["-f", "hpl_CUDA", "-m", "2", "-b", "5", "--uniform", "--precision", "bf16"])
     assert r.returncode == 1
     assert "pivoting" in r.stderr
