@@ -249,6 +249,61 @@ def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
 FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
 
 
+def run_fp64(ctx, lp, torch, stream, A, b64, n, steps, warmup, peak_fp64) -> dict:
+    """The double build (DATA_TYPE double): the same system's FP32 entries
+    widened to double, b in double (x = ones exactly); a step = restore A,
+    lp_gefa_f64_dev (bs 128) + lp_gesl_f64_dev, on device time."""
+    bs = 128
+    with torch.cuda.stream(stream):
+        dA0 = torch.from_numpy(A).to("cuda").double()
+        db0 = torch.from_numpy(b64).to("cuda")
+        dA = torch.empty_like(dA0)
+        dB = torch.empty_like(db0)
+    torch.cuda.synchronize()
+
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+            dB.copy_(db0)
+        ctx.gefa_f64(dA.data_ptr(), n, n, bs)
+        ctx.gesl_f64(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
+
+    for _ in range(warmup):
+        step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.read_profile(reset=True)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    prof = ctx.read_profile(reset=True)
+    ctx.set_profiling(False)
+    resid = float((dB - 1.0).abs().max())
+    normb = float(db0.abs().max())
+    inner = prof["inner"]
+    tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
+    stage_s = {k: prof[k]["s"] for k in lp.STAGES if prof[k]["calls"]}
+    tot = sum(stage_s.values())
+    del dA0, dA
+    return {
+        "workload": f"FP64 LU without pivoting + substitution (the double build), n={n}, block {bs}, the FP32 "
+                    "workload's entries widened to double, b = A*ones in double",
+        "value": steps * flops(n) / t / 1e9, "unit": UNIT, "ms_per_step": 1e3 * t / steps,
+        "max_abs_err_x": resid, "residn_dbl": resid / (n * normb * float(np.finfo(np.float64).eps)),
+        "roofline": {"bound": "fp64_simt", "kernel": "k_dgemm_update (inner stage)", "achieved": tfs,
+                     "peak": peak_fp64, "unit": "TFLOP/s", "frac": tfs / peak_fp64 if tfs else None,
+                     "peak_source": "derived: 148 SMs x 64 FP64 lanes x 2 flop x median SM clock under load"},
+        "stages": {k: {"s": v, "share": v / tot if tot > 0 else None, "calls": prof[k]["calls"]}
+                   for k, v in stage_s.items()},
+    }
+
+
 def run_pivot(ctx, lp, torch, stream, n, steps, warmup, pk) -> dict:
     """LU with partial pivoting (the harness's --uniform case, gefa_ref /
     gesl_ref convention) on a non-dominant matrix: U(0,1) entries (seed 42,
@@ -397,6 +452,7 @@ def main() -> None:
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-pivot", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--serve-rates", default="100,200,300,400,500,600,700,800,900,1000,1250,1500,2000,5000,20000")
     ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
@@ -498,6 +554,11 @@ def main() -> None:
             pivot["roofline"]["peak"] = peak_tf
             pivot["roofline"]["frac"] = pivot["roofline"]["achieved"] / peak_tf
 
+    fp64 = None
+    if not args.no_fp64 and n % 128 == 0:
+        fp64 = run_fp64(ctx, lp, torch, stream, A, b64, n, args.steps, max(1, min(args.warmup, 2)),
+                        NUM_SMS * 64 * 2 * sm_mhz * 1e6 / 1e12)
+
     batched = None
     if not args.no_batch:
         batched = run_batched(ctx, lp, torch, stream, args.steps, max(1, min(args.warmup, 2)), args.batch_count)
@@ -579,6 +640,8 @@ def main() -> None:
         line["mixed"] = mixed
     if pivot is not None:
         line["pivot"] = pivot
+    if fp64 is not None:
+        line["fp64"] = fp64
     if batched is not None:
         line["batched"] = batched
     if serving is not None:

@@ -123,10 +123,11 @@ __global__ void __launch_bounds__(PT, 1)
     const int row0 = g * R;                       // M rows k0 + row0 ... belong to this CTA
     const int nr = max(0, min(R, n - k0 - row0));
     const size_t cbase = (size_t)k0 + row0;       // their storage column
-    for (int c = 0; c < kb; c++) {
+    for (int c = 0; c < kb; c++) {  // every copy in flight before the first wait
         const float* src = a + (size_t)(k0 + c) * lda + cbase;
-        for (int r = tid; r < nr; r += PT) slab[c * R + r] = src[r];
+        for (int r = tid; r < nr; r += PT) cp_async4(slab + c * R + r, src + r);
     }
+    cp_async_wait_all();
     __syncthreads();
     for (int kk = 0; kk < kb; kk++) {
         const int k = k0 + kk, par = kk & 1;
@@ -275,8 +276,9 @@ __global__ void __launch_bounds__(PT)
     for (int t = tid; t < PB; t += PT) pv[t] = ipvt[k0 + t];
     for (int idx = tid; idx < PB * PB; idx += PT) {
         const int k = idx / PB, t = idx - k * PB;
-        L[idx] = a[(size_t)(k0 + k) * lda + k0 + t];
+        cp_async4(L + idx, a + (size_t)(k0 + k) * lda + k0 + t);
     }
+    cp_async_wait_all();
     __syncthreads();
     if (warp == 0) build_perm(pv, k0, PB, r0, psrc, odst, osrc, &s_nout);
     __syncthreads();
@@ -374,6 +376,22 @@ __global__ void k_piv_convert(float* __restrict__ a, int lda, int n, int pb, con
     }
 }
 
+// acc + sgn * sum_{t < kb} ys[t] * S[k0 + t][i] in ascending t, the column
+// read 16 rows at a time with all 16 loads in flight before they are used.
+__device__ __forceinline__ float panel_dot(const float* __restrict__ a, int lda, int k0, int kb, int i,
+                                           const float* ys, float sgn, float acc) {
+    const float* col = a + (size_t)k0 * lda + i;
+    for (int t0 = 0; t0 < kb; t0 += 16) {
+        float v[16];
+#pragma unroll
+        for (int j = 0; j < 16; j++) v[j] = t0 + j < kb ? __ldg(col + (size_t)(t0 + j) * lda) : 0.0f;
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+            if (t0 + j < kb) acc = fmaf(sgn * ys[t0 + j], v[j], acc);
+    }
+    return acc;
+}
+
 // Forward and back substitution on block-form factors, nrhs right-hand
 // sides (rows of b, solutions overwrite them).  w: 3 n floats (the forward
 // values y, two alternating trailing vectors).  Per panel every CTA computes
@@ -412,8 +430,9 @@ __global__ void __launch_bounds__(PT, 1)
             if (tid == 0) s_nout = dj[3 * PB];
             for (int idx = tid; idx < kb * kb; idx += PT) {
                 const int k = idx / kb, t = idx - k * kb;
-                D[k * PB + t] = a[(size_t)(k0 + k) * lda + k0 + t];
+                cp_async4(D + k * PB + t, a + (size_t)(k0 + k) * lda + k0 + t);
             }
+            cp_async_wait_all();
             const int mrest = n - r0, ch = (mrest + G - 1) / G, i0 = r0 + g * ch, i1 = min(n, i0 + ch);
             for (int i = tid; i < ch; i += PT) ovr[i] = -1;
             __syncthreads();
@@ -450,9 +469,7 @@ __global__ void __launch_bounds__(PT, 1)
             __syncthreads();
             for (int i = i0 + tid; i < i1; i += PT) {
                 const int o = ovr[i - i0];
-                float acc = __ldcg(cur + (o >= 0 ? o : i));
-                for (int t = 0; t < kb; t++) acc = fmaf(ys[t], a[(size_t)(k0 + t) * lda + i], acc);
-                nxt[i] = acc;
+                nxt[i] = panel_dot(a, lda, k0, kb, i, ys, 1.0f, __ldcg(cur + (o >= 0 ? o : i)));
             }
             if (!grid_sync(bar, (++nbar) * (unsigned)G, err)) return;
         }
@@ -461,8 +478,9 @@ __global__ void __launch_bounds__(PT, 1)
             const int k0 = j * PB, kb = min(PB, n - k0);
             for (int idx = tid; idx < kb * kb; idx += PT) {
                 const int k = idx / kb, t = idx - k * kb;
-                D[k * PB + t] = a[(size_t)(k0 + k) * lda + k0 + t];
+                cp_async4(D + k * PB + t, a + (size_t)(k0 + k) * lda + k0 + t);
             }
+            cp_async_wait_all();
             __syncthreads();
             if (warp == 0) {
                 float x[Q];
@@ -494,11 +512,7 @@ __global__ void __launch_bounds__(PT, 1)
             }
             __syncthreads();
             const int ch = (k0 + G - 1) / G, i0 = g * ch, i1 = min(k0, i0 + ch);
-            for (int i = i0 + tid; i < i1; i += PT) {
-                float acc = __ldcg(y + i);
-                for (int t = 0; t < kb; t++) acc = fmaf(-ys[t], a[(size_t)(k0 + t) * lda + i], acc);
-                y[i] = acc;
-            }
+            for (int i = i0 + tid; i < i1; i += PT) y[i] = panel_dot(a, lda, k0, kb, i, ys, -1.0f, __ldcg(y + i));
             if (!grid_sync(bar, (++nbar) * (unsigned)G, err)) return;
         }
     }

@@ -154,40 +154,41 @@ __global__ void __launch_bounds__(kTrsmThreads) k_trsm_left(const float* __restr
 // multiply and add.  Same per-element operation sequence as above.
 constexpr int kCW = 32;  // columns (top) / rows (left) per CTA
 
-template <int BS>
-__global__ void __launch_bounds__(kTrsmThreads) k_top_chunk(const float* __restrict__ lu, int ldlu,
-                                                          float* __restrict__ t, int ldt, int ncols) {
+template <typename E, int BS>
+__global__ void __launch_bounds__(kTrsmThreads) k_top_chunk(const E* __restrict__ lu, int ldlu,
+                                                          E* __restrict__ t, int ldt, int ncols) {
+    using R = Rn<E>;
     constexpr int NB = BS < 32 ? BS : 32;
     constexpr int SL = BS + 4, TL = kCW + 4;
-    extern __shared__ __align__(16) float sm[];
-    float* D = sm;             // BS x SL: the factored diagonal block
-    float* T = sm + BS * SL;   // BS x TL: the CTA's columns
+    extern __shared__ __align__(16) unsigned char trsm_raw[];
+    E* D = reinterpret_cast<E*>(trsm_raw);  // BS x SL: the factored diagonal block
+    E* T = D + BS * SL;                     // BS x TL: the CTA's columns
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c0 = blockIdx.x * kCW;
     for (int idx = tid; idx < BS * BS; idx += kTrsmThreads) {
         const int j = idx / BS, k = idx - j * BS;
-        cp_async4(D + j * SL + k, lu + (size_t)j * ldlu + k);
+        cp_async_elem(D + j * SL + k, lu + (size_t)j * ldlu + k);
     }
     for (int idx = tid; idx < BS * kCW; idx += kTrsmThreads) {
         const int r = idx / kCW, cc = idx - r * kCW;
         if (c0 + cc < ncols)
-            cp_async4(T + r * TL + cc, t + (size_t)r * ldt + c0 + cc);
+            cp_async_elem(T + r * TL + cc, t + (size_t)r * ldt + c0 + cc);
         else
-            T[r * TL + cc] = 0.0f;
+            T[r * TL + cc] = E(0);
     }
     cp_async_wait_all();
     __syncthreads();
     for (int k0 = 0; k0 < BS; k0 += NB) {
         if (warp == 0) {  // rows k0..k0+NB-1 of column `lane`: t_k *= D_kk; t_j += t_k D_jk
-            float x[NB];
+            E x[NB];
 #pragma unroll
             for (int j = 0; j < NB; j++) x[j] = T[(k0 + j) * TL + lane];
 #pragma unroll
             for (int k = 0; k < NB; k++) {
-                x[k] = __fmul_rn(x[k], D[(k0 + k) * SL + k0 + k]);
+                x[k] = R::mul(x[k], D[(k0 + k) * SL + k0 + k]);
 #pragma unroll
                 for (int j = k + 1; j < NB; j++)
-                    x[j] = __fadd_rn(x[j], __fmul_rn(x[k], D[(k0 + j) * SL + k0 + k]));
+                    x[j] = R::add(x[j], R::mul(x[k], D[(k0 + j) * SL + k0 + k]));
             }
 #pragma unroll
             for (int j = 0; j < NB; j++) T[(k0 + j) * TL + lane] = x[j];
@@ -196,26 +197,26 @@ __global__ void __launch_bounds__(kTrsmThreads) k_top_chunk(const float* __restr
         const int base = k0 + NB;
         if (base == BS) break;
         // rows below the chunk: T[r][c] += sum_kk T[k0+kk][c] D[r][k0+kk]; two rows per pass
-        float tv[NB];
+        E tv[NB];
 #pragma unroll
         for (int kk = 0; kk < NB; kk++) tv[kk] = T[(k0 + kk) * TL + lane];
         for (int r = base + warp; r < BS; r += 16) {
             const int r2 = r + 8;  // (BS - base) / 8 is even
-            float acc = T[r * TL + lane], acc2 = T[r2 * TL + lane];
-            const float* d1 = D + r * SL + k0;
-            const float* d2 = D + r2 * SL + k0;
+            E acc = T[r * TL + lane], acc2 = T[r2 * TL + lane];
+            const E* d1 = D + r * SL + k0;
+            const E* d2 = D + r2 * SL + k0;
 #pragma unroll
             for (int kk = 0; kk < NB; kk += 4) {
-                const float4 u = *reinterpret_cast<const float4*>(d1 + kk);
-                const float4 v = *reinterpret_cast<const float4*>(d2 + kk);
-                acc = __fadd_rn(acc, __fmul_rn(tv[kk], u.x));
-                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk], v.x));
-                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 1], u.y));
-                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 1], v.y));
-                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 2], u.z));
-                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 2], v.z));
-                acc = __fadd_rn(acc, __fmul_rn(tv[kk + 3], u.w));
-                acc2 = __fadd_rn(acc2, __fmul_rn(tv[kk + 3], v.w));
+                const Quad<E> u = ld_quad(d1 + kk);
+                const Quad<E> v = ld_quad(d2 + kk);
+                acc = R::add(acc, R::mul(tv[kk], u.x));
+                acc2 = R::add(acc2, R::mul(tv[kk], v.x));
+                acc = R::add(acc, R::mul(tv[kk + 1], u.y));
+                acc2 = R::add(acc2, R::mul(tv[kk + 1], v.y));
+                acc = R::add(acc, R::mul(tv[kk + 2], u.z));
+                acc2 = R::add(acc2, R::mul(tv[kk + 2], v.z));
+                acc = R::add(acc, R::mul(tv[kk + 3], u.w));
+                acc2 = R::add(acc2, R::mul(tv[kk + 3], v.w));
             }
             T[r * TL + lane] = acc;
             T[r2 * TL + lane] = acc2;
@@ -228,40 +229,41 @@ __global__ void __launch_bounds__(kTrsmThreads) k_top_chunk(const float* __restr
     }
 }
 
-template <int BS>
-__global__ void __launch_bounds__(kTrsmThreads) k_left_chunk(const float* __restrict__ lu, int ldlu,
-                                                           float* __restrict__ l, int ldl, int nrows,
-                                                           float* __restrict__ lt, int ldlt) {
+template <typename E, int BS>
+__global__ void __launch_bounds__(kTrsmThreads) k_left_chunk(const E* __restrict__ lu, int ldlu,
+                                                           E* __restrict__ l, int ldl, int nrows,
+                                                           E* __restrict__ lt, int ldlt) {
+    using R = Rn<E>;
     constexpr int NB = BS < 32 ? BS : 32;
     constexpr int SL = BS + 4;
-    extern __shared__ __align__(16) float sm[];
-    float* D = sm;             // BS x SL: the factored diagonal block
-    float* L = sm + BS * SL;   // kCW x SL: the CTA's rows
+    extern __shared__ __align__(16) unsigned char trsm_raw[];
+    E* D = reinterpret_cast<E*>(trsm_raw);  // BS x SL: the factored diagonal block
+    E* L = D + BS * SL;                     // kCW x SL: the CTA's rows
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int r0 = blockIdx.x * kCW;
     for (int idx = tid; idx < BS * BS; idx += kTrsmThreads) {
         const int k = idx / BS, i = idx - k * BS;
-        cp_async4(D + k * SL + i, lu + (size_t)k * ldlu + i);
+        cp_async_elem(D + k * SL + i, lu + (size_t)k * ldlu + i);
     }
     for (int idx = tid; idx < kCW * BS; idx += kTrsmThreads) {
         const int r = idx / BS, c = idx - r * BS;
         if (r0 + r < nrows)
-            cp_async4(L + r * SL + c, l + (size_t)(r0 + r) * ldl + c);
+            cp_async_elem(L + r * SL + c, l + (size_t)(r0 + r) * ldl + c);
         else
-            L[r * SL + c] = 0.0f;
+            L[r * SL + c] = E(0);
     }
     cp_async_wait_all();
     __syncthreads();
     for (int k0 = 0; k0 < BS; k0 += NB) {
         if (warp == 0) {  // columns k0..k0+NB-1 of row `lane`: l_i += l_k D_ki (i > k)
-            float x[NB];
+            E x[NB];
 #pragma unroll
             for (int i = 0; i < NB; i++) x[i] = L[lane * SL + k0 + i];
 #pragma unroll
             for (int k = 0; k < NB; k++)
 #pragma unroll
                 for (int i = k + 1; i < NB; i++)
-                    x[i] = __fadd_rn(x[i], __fmul_rn(x[k], D[(k0 + k) * SL + k0 + i]));
+                    x[i] = R::add(x[i], R::mul(x[k], D[(k0 + k) * SL + k0 + i]));
 #pragma unroll
             for (int i = 0; i < NB; i++) L[lane * SL + k0 + i] = x[i];
         }
@@ -271,21 +273,21 @@ __global__ void __launch_bounds__(kTrsmThreads) k_left_chunk(const float* __rest
         // columns after the chunk: L[r][i] += sum_kk L[r][k0+kk] D[k0+kk][i]; lane = column, warp = row
         for (int g = 0; g < (BS - base) / 32; g++) {
             const int i = base + 32 * g + lane;
-            float dv[NB];
+            E dv[NB];
 #pragma unroll
             for (int kk = 0; kk < NB; kk++) dv[kk] = D[(k0 + kk) * SL + i];
-            float acc[kCW / 8];
+            E acc[kCW / 8];
 #pragma unroll
             for (int s = 0; s < kCW / 8; s++) acc[s] = L[(warp + 8 * s) * SL + i];
 #pragma unroll
             for (int kk = 0; kk < NB; kk += 4) {
 #pragma unroll
                 for (int s = 0; s < kCW / 8; s++) {
-                    const float4 u = *reinterpret_cast<const float4*>(L + (warp + 8 * s) * SL + k0 + kk);
-                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.x, dv[kk]));
-                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.y, dv[kk + 1]));
-                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.z, dv[kk + 2]));
-                    acc[s] = __fadd_rn(acc[s], __fmul_rn(u.w, dv[kk + 3]));
+                    const Quad<E> u = ld_quad(L + (warp + 8 * s) * SL + k0 + kk);
+                    acc[s] = R::add(acc[s], R::mul(u.x, dv[kk]));
+                    acc[s] = R::add(acc[s], R::mul(u.y, dv[kk + 1]));
+                    acc[s] = R::add(acc[s], R::mul(u.z, dv[kk + 2]));
+                    acc[s] = R::add(acc[s], R::mul(u.w, dv[kk + 3]));
                 }
             }
 #pragma unroll
@@ -304,19 +306,20 @@ __global__ void __launch_bounds__(kTrsmThreads) k_left_chunk(const float* __rest
     }
 }
 
-template <int BS>
-constexpr size_t top_chunk_smem() { return sizeof(float) * ((size_t)BS * (BS + 4) + (size_t)BS * (kCW + 4)); }
-template <int BS>
-constexpr size_t left_chunk_smem() { return sizeof(float) * ((size_t)BS * (BS + 4) + (size_t)kCW * (BS + 4)); }
+template <typename E, int BS>
+constexpr size_t top_chunk_smem() { return sizeof(E) * ((size_t)BS * (BS + 4) + (size_t)BS * (kCW + 4)); }
+template <typename E, int BS>
+constexpr size_t left_chunk_smem() { return sizeof(E) * ((size_t)BS * (BS + 4) + (size_t)kCW * (BS + 4)); }
 
-template <int BS>
-void launch_left_chunk(const float* lu, int ldlu, float* l, int ldl, int nrows, float* lt, int ldlt, cudaStream_t st) {
-    k_left_chunk<BS><<<(nrows + kCW - 1) / kCW, kTrsmThreads, left_chunk_smem<BS>(), st>>>(lu, ldlu, l, ldl, nrows,
-                                                                                          lt, ldlt);
+template <int BS, typename E>
+void launch_left_chunk(const E* lu, int ldlu, E* l, int ldl, int nrows, E* lt, int ldlt, cudaStream_t st) {
+    k_left_chunk<E, BS><<<(nrows + kCW - 1) / kCW, kTrsmThreads, left_chunk_smem<E, BS>(), st>>>(lu, ldlu, l, ldl,
+                                                                                                nrows, lt, ldlt);
 }
-template <int BS>
-void launch_top_chunk(const float* lu, int ldlu, float* t, int ldt, int ncols, cudaStream_t st) {
-    k_top_chunk<BS><<<(ncols + kCW - 1) / kCW, kTrsmThreads, top_chunk_smem<BS>(), st>>>(lu, ldlu, t, ldt, ncols);
+template <int BS, typename E>
+void launch_top_chunk(const E* lu, int ldlu, E* t, int ldt, int ncols, cudaStream_t st) {
+    k_top_chunk<E, BS><<<(ncols + kCW - 1) / kCW, kTrsmThreads, top_chunk_smem<E, BS>(), st>>>(lu, ldlu, t, ldt,
+                                                                                               ncols);
 }
 
 int log2i(int x) {
@@ -336,10 +339,45 @@ int trsm_init_attrs() {
     LP_CUDA(cudaFuncSetAttribute(k_trsm_top<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)top_smem(512, 16)));
     LP_CUDA(cudaFuncSetAttribute(k_trsm_left<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
     LP_CUDA(cudaFuncSetAttribute(k_trsm_left<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)left_smem(512, 16)));
-    LP_CUDA(cudaFuncSetAttribute(k_left_chunk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)left_chunk_smem<128>()));
-    LP_CUDA(cudaFuncSetAttribute(k_top_chunk<128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)top_chunk_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_left_chunk<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)left_chunk_smem<float, 128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_top_chunk<float, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)top_chunk_smem<float, 128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_left_chunk<double, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)left_chunk_smem<double, 128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_top_chunk<double, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)top_chunk_smem<double, 128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_left_chunk<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)left_chunk_smem<double, 64>()));
+    LP_CUDA(cudaFuncSetAttribute(k_top_chunk<double, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)top_chunk_smem<double, 64>()));
+    return LP_OK;
+}
+
+int launch_top_chunk_f64(const double* lu, int ldlu, double* t, int ldt, int bs, int ncols, cudaStream_t st) {
+    if (ncols <= 0) return LP_OK;
+    if (bs == 128)
+        launch_top_chunk<128>(lu, ldlu, t, ldt, ncols, st);
+    else if (bs == 64)
+        launch_top_chunk<64>(lu, ldlu, t, ldt, ncols, st);
+    else
+        return fail(LP_E_INVALID, "FP64 top update: bs must be 64 or 128");
+    count_launch();
+    LP_CUDA(cudaGetLastError());
+    return LP_OK;
+}
+
+int launch_left_chunk_f64(const double* lu, int ldlu, double* l, int ldl, int bs, int nrows, double* lt, int ldlt,
+                          cudaStream_t st) {
+    if (nrows <= 0) return LP_OK;
+    if (bs == 128)
+        launch_left_chunk<128>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+    else if (bs == 64)
+        launch_left_chunk<64>(lu, ldlu, l, ldl, nrows, lt, ldlt, st);
+    else
+        return fail(LP_E_INVALID, "FP64 left update: bs must be 64 or 128");
+    count_launch();
+    LP_CUDA(cudaGetLastError());
     return LP_OK;
 }
 

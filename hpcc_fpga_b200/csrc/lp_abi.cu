@@ -348,6 +348,7 @@ int lp_ctx_create(int device, lp_ctx** out) {
     LP_CHECK(umma_init_attrs());
     LP_CHECK(batch_init_attrs());
     LP_CHECK(piv_init_attrs());
+    LP_CHECK(dgemm_init_attrs());
     lp_ctx* c = new lp_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;

@@ -41,11 +41,57 @@ __device__ __forceinline__ void cp_async4(float* smem, const float* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// 8-byte copy of one double.
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_elem(float* smem, const float* gmem) { cp_async4(smem, gmem); }
+__device__ __forceinline__ void cp_async_elem(double* smem, const double* gmem) { cp_async8(smem, gmem); }
+
+// Separately rounded product and sum, and -1/x correctly rounded, in the
+// element type: the reference's host arithmetic without fused multiply-add
+// (for float, -1.0/x divided in double and rounded to float equals the
+// correctly rounded float reciprocal, negated).
+template <typename T>
+struct Rn;
+template <>
+struct Rn<float> {
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float neg_rcp(float a) { return -__frcp_rn(a); }
+};
+template <>
+struct Rn<double> {
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double neg_rcp(double a) { return -__drcp_rn(a); }
+};
+
+// Four consecutive elements from 16-byte aligned shared memory.
+template <typename T>
+struct Quad {
+    T x, y, z, w;
+};
+__device__ __forceinline__ Quad<float> ld_quad(const float* p) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Quad<double> ld_quad(const double* p) {
+    const double2 a = *reinterpret_cast<const double2*>(p);
+    const double2 b = *reinterpret_cast<const double2*>(p + 2);
+    return {a.x, a.y, b.x, b.y};
+}
 #endif
 
 // ---- kernel launchers (each returns LP_OK or an error status) ------------
 // Diagonal block LU for bs <= 128, whole block in shared memory.
 int launch_lu_small(float* a, int lda, int bs, cudaStream_t s);
+// The same kernels on FP64 blocks (bs 64 or 128): the reference's _DP build.
+int launch_lu_small_f64(double* a, int lda, int bs, cudaStream_t s);
+int launch_top_chunk_f64(const double* lu, int ldlu, double* t, int ldt, int bs, int ncols, cudaStream_t s);
+int launch_left_chunk_f64(const double* lu, int ldlu, double* l, int ldl, int bs, int nrows, double* lt, int ldlt,
+                          cudaStream_t s);
 // Triangular block updates (top: column-independent; left: row-independent).
 int launch_trsm_top(const float* lu, int ldlu, float* t, int ldt, int bs, int ncols, cudaStream_t s);
 int launch_trsm_left(const float* lu, int ldlu, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
@@ -53,6 +99,10 @@ int launch_trsm_left(const float* lu, int ldlu, float* l, int ldl, int bs, int n
 // FP32 SIMT trailing update C(m x n) += Lt^T (bs x m) * T (bs x n).
 int launch_sgemm_update(float* c, int ldc, const float* lt, int ldlt, const float* t, int ldt, int m, int n,
                         int k, cudaStream_t s);
+// FP64 SIMT trailing update, the same operand layout (k_dgemm.cu).
+int launch_dgemm_update(double* c, int ldc, const double* lt, int ldlt, const double* t, int ldt, int m, int n, int k,
+                        cudaStream_t s);
+int dgemm_init_attrs();
 int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t s);
 // Forward + back substitution for nrhs rows of b (see k_gesl.cu).
 int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t s);

@@ -47,6 +47,9 @@ constexpr int kBatchSolveOnly = 1 << 8;
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
                 int max_iters, int* iters, double* resid, cudaStream_t st);
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
+// FP64 form (lp_fp64.cu): factorization and substitution in double.
+int gefa_f64(lp_ctx* c, double* a, int n, int lda, int bs, cudaStream_t st);
+int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st);
 // Partial pivoting (k_pivot.cu): kernels of the blocked LINPACK-convention LU.
 int piv_init_attrs();
 size_t piv_sync_bytes();
@@ -95,6 +98,7 @@ struct lp_ctx {
     lp::Workspace dnorm;                      // refinement norms (device)
     unsigned long long* hnorm = nullptr;      // their pinned host copy
     size_t hnorm_cap = 0;
+    lp::Workspace f64a, f64b, f64lt, f64w;  // FP64: host-entry matrix and rhs, transposed left panel, solve vectors
     lp::Workspace psync, pat, pdesc, pw, pipvt;  // pivoting: barrier + exchange area, transposed U12,
                                                  // interchange permutations, solve vectors, ipvt
     lp::Workspace bsys, bnext;                // batched: sorted system descriptors, work counter
@@ -114,7 +118,7 @@ struct lp_ctx {
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
         lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
-                                &dnorm, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
+                                &dnorm, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
         bgraph = nullptr;

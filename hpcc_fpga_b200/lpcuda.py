@@ -169,6 +169,9 @@ def lib() -> ctypes.CDLL:
     L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
     L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
+    L.lp_gefa_f64_dev.argtypes = [_VP, _VP, _I, _I, _I]
+    L.lp_gesl_f64_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
+    L.lp_calculate_f64.argtypes = [_VP, _I, _I, _I, _I, _F64P, _F64P, _F64P, _F64P]
     L.lp_gefa_pvt_dev.argtypes = [_VP, _VP, _I, _I, _VP]
     L.lp_gesl_pvt_dev.argtypes = [_VP, _VP, _I, _I, _VP, _VP, _I, _I]
     L.lp_calculate_pvt.argtypes = [_VP, _I, _I, _I, _F32P, _F32P, _I32P, _F64P, _F64P]
@@ -333,6 +336,21 @@ class Context:
 
     def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
         check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")
+
+    # ---- FP64 (the reference's double build) ----------------------------------
+    def gefa_f64(self, dA: int, n: int, lda: int, bs: int = 128) -> None:
+        check(lib().lp_gefa_f64_dev(self._h, dA, n, lda, bs), "lp_gefa_f64_dev")
+
+    def gesl_f64(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
+        check(lib().lp_gesl_f64_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_f64_dev")
+
+    def calculate_f64(self, A: np.ndarray, b: np.ndarray, bs: int = 128, repetitions: int = 1):
+        """Double build of the backend: A (float64) -> factors, b -> x."""
+        n = A.shape[0]
+        tg = np.zeros(repetitions, np.float64)
+        ts = np.zeros(repetitions, np.float64)
+        check(lib().lp_calculate_f64(self._h, n, A.shape[1], bs, repetitions, A, b, tg, ts), "lp_calculate_f64")
+        return {"gefa": tg.tolist(), "gesl": ts.tolist()}
 
     # ---- partial pivoting (gefa_ref / gesl_ref) -------------------------------
     def gefa_pvt(self, dA: int, n: int, lda: int, dIpvt: int) -> None:

@@ -1,5 +1,6 @@
 /*
- * lpcuda — B200 (sm_100a) LINPACK LU-without-pivoting + substitution.
+ * lpcuda — B200 (sm_100a) LINPACK LU-without-pivoting + substitution, with the
+ * reference's partial-pivoting and double-precision variants.
  *
  * C ABI of liblpcuda.so: plain pointers and sizes, no C++ types, no
  * exceptions.  Every entry point returns an int status (LP_OK = 0, < 0 on
@@ -195,6 +196,15 @@ int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nr
  * lp_gesl_dev; the solutions overwrite dB. */
 int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, void* stream);
 
+/* ---- FP64 (the reference's _DP build; device pointers) --------------------
+ * The same blocked LU without pivoting and the same encoding in double
+ * (DATA_TYPE / HOST_DATA_TYPE double, LINPACK/src/host/parameters.h.in):
+ * gefa_ref_nopvt / gesl_ref_nopvt of the double build.  bs 64 or 128, n a
+ * multiple of bs, lda even, dA 16-byte aligned. */
+int lp_gefa_f64_dev(lp_ctx* ctx, double* dA, int n, int lda, int bs);
+/* Forward + back substitution, nrhs right-hand sides as rows of dB. */
+int lp_gesl_f64_dev(lp_ctx* ctx, const double* dLU, int n, int lda, double* dB, int nrhs, int ldb);
+
 /* ---- LU with partial pivoting (device pointers) ------------------------------
  * The reference's gefa_ref / gesl_ref (LINPACK/src/host/linpack_data.cpp:72-156),
  * which its harness uses for matrices that are not diagonally dominant
@@ -225,6 +235,10 @@ int lp_gesl_pvt_dev(lp_ctx* ctx, float* dLU, int n, int lda, const int* dIpvt, f
  * linpack_benchmark.hpp:321-323), b holds the solution x. */
 int lp_calculate(lp_ctx* ctx, int n, int lda, int bs, int repetitions, float* A, float* b,
                  double* gefa_times, double* gesl_times);
+/* The same backend for the double build: A, b in double, factors in
+ * gefa_ref_nopvt<double>'s encoding, b -> x. */
+int lp_calculate_f64(lp_ctx* ctx, int n, int lda, int bs, int repetitions, double* A, double* b,
+                     double* gefa_times, double* gesl_times);
 /* The same backend for matrices that are not diagonally dominant (the
  * harness's --uniform case): partial pivoting, LINPACK convention.  On return
  * A holds the factors in gefa_ref's encoding, ipvt (n entries) the pivots,
