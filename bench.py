@@ -178,6 +178,58 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, 
     }
 
 
+def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, steps, warmup, f32_value, pk) -> dict:
+    """FP32 emulated on the BF16 tensor cores (LP_F32_BF16X6: exact three-term
+    BF16 split of every operand, six products, FP32 accumulation) on the same
+    system and the same step as the FP32 headline: restore A and b, factor,
+    plain FP32 solve — no refinement."""
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+            dB.copy_(dB0)
+        ctx.gefa_prec("f32_bf16x6", dA.data_ptr(), n, n, bs)
+        ctx.gesl(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
+
+    for _ in range(warmup):
+        step()
+    ctx.sync()
+    ctx.set_profiling(True)
+    ctx.read_profile(reset=True)
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    prof = ctx.read_profile(reset=True)
+    ctx.set_profiling(False)
+    x = dB.cpu().numpy().astype(np.float64)
+    with torch.cuda.stream(stream):
+        dB64 = torch.from_numpy(b64).to("cuda")
+        dXr = torch.empty(n, dtype=torch.float64, device="cuda")
+    r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
+    inner = prof["inner"]
+    tf32eq = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
+    value = steps * flops(n) / t / 1e9
+    return {
+        "workload": f"the FP32 workload (n={n}, block {bs}, same system and step) with the trailing update "
+                    "emulated on the BF16 tensor cores: exact 3-term BF16 split, 6 products, FP32 accumulation; "
+                    "plain FP32 solve, no refinement",
+        "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32_simt": value / f32_value,
+        "max_abs_err_x": float(np.abs(x - 1.0).max()),
+        "hpl_resid": {"eps_flt_half": r32 * 2.0 ** -29, "eps_dbl_half": r32},
+        "roofline": {"bound": "tensor", "kernel": "k_umma_update (inner stage, K = 6 bs)",
+                     "achieved": 6 * tf32eq if tf32eq else None, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                     "frac": 6 * tf32eq / pk["bf16_tflops"] if tf32eq else None,
+                     "fp32_equivalent_tflops": tf32eq, "peak_source": pk["source"],
+                     "per_unit": "6 x 2*m*n*bs BF16 flop per m x n trailing update (2*m*n*bs FP32-equivalent)"},
+        "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]},
+    }
+
+
 def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
     """The batched workload: `count` systems, n log-uniform in [32, 1024]
     (seed 7), 1..8 right-hand sides, seeded diagonally dominant matrices; one
@@ -453,6 +505,7 @@ def main() -> None:
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-pivot", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-f32emu", action="store_true")
     ap.add_argument("--serve-rates", default="100,200,300,400,500,600,700,800,900,1000,1250,1500,2000,5000,20000")
     ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
@@ -547,6 +600,11 @@ def main() -> None:
             mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, args.steps,
                                     max(1, min(args.warmup, 2)), value / world, pk)
 
+    f32emu = None
+    if not args.no_f32emu and bs % 128 == 0:
+        f32emu = run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, args.steps,
+                            max(1, min(args.warmup, 2)), value / world, pk)
+
     pivot = None
     if not args.no_pivot:
         pivot = run_pivot(ctx, lp, torch, stream, n, args.steps, max(1, min(args.warmup, 2)), pk)
@@ -638,6 +696,8 @@ def main() -> None:
     }
     if mixed:
         line["mixed"] = mixed
+    if f32emu is not None:
+        line["f32_bf16x6"] = f32emu
     if pivot is not None:
         line["pivot"] = pivot
     if fp64 is not None:

@@ -8,6 +8,13 @@
 //          and the update adds s_L * s_T * (Lq Tq^T) in FP32.
 // The FP32 factors the substitution uses are these rounded-update factors;
 // accuracy is recovered by FP64 iterative refinement (lp_solve.cu).
+//   BF16x6 (FP32 emulation): every element x of L and T is split exactly into
+//          three BF16 terms x1 = bf16(x), x2 = bf16(x - x1), x3 = x - x1 - x2
+//          (8 + 8 + 8 significant bits = the 24 of an FP32), and the operands
+//          become six K-segments so that one tensor-core GEMM with K = 6 bs
+//          accumulates x3 t1 + x2 t2 + x1 t3 + x2 t1 + x1 t2 + x1 t1 in FP32
+//          (small terms first).  The three dropped products (x2 t3, x3 t2,
+//          x3 t3) are below 2^-24 of x1 t1: the update has FP32 accuracy.
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
 
@@ -100,7 +107,74 @@ __global__ void __launch_bounds__(256) k_quant_trans(const float* __restrict__ T
     }
 }
 
+// Exact three-term BF16 split of an FP32 value (each remainder is exact in FP32).
+__device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16& b, __nv_bfloat16& c) {
+    a = __float2bfloat16_rn(x);
+    const float r1 = x - __bfloat162float(a);
+    b = __float2bfloat16_rn(r1);
+    c = __float2bfloat16_rn(r1 - __bfloat162float(b));
+}
+
+// Segment s of the K = 6 k operand row pairs L-term kLseg[s] with T-term kTseg[s].
+__constant__ int kLseg[6] = {2, 1, 0, 1, 0, 0};
+__constant__ int kTseg[6] = {0, 1, 2, 0, 1, 0};
+
+// out[r][s*k + c] = term kLseg[s] of L[r][c]: rows x (6 k) BF16.
+__global__ void k_split_rows(const float* __restrict__ L, int ldl, __nv_bfloat16* __restrict__ out, int rows, int k) {
+    const size_t total = (size_t)rows * k;
+    const size_t kq = 6 * (size_t)k;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / k), c = (int)(e - (size_t)r * k);
+        __nv_bfloat16 t[3];
+        split3(L[(size_t)r * ldl + c], t[0], t[1], t[2]);
+        __nv_bfloat16* o = out + (size_t)r * kq + c;
+#pragma unroll
+        for (int s = 0; s < 6; s++) o[(size_t)s * k] = t[kLseg[s]];
+    }
+}
+
+// out[c][s*k + r] = term kTseg[s] of T[r][c]: cols x (6 k) BF16, through a
+// 32 x 32 shared-memory transpose.
+__global__ void __launch_bounds__(256) k_split_trans(const float* __restrict__ T, int ldt,
+                                                     __nv_bfloat16* __restrict__ out, int k, int cols) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int r = r0 + ty + j, c = c0 + tx;
+        tile[ty + j][tx] = (r < k && c < cols) ? T[(size_t)r * ldt + c] : 0.0f;
+    }
+    __syncthreads();
+    const size_t kq = 6 * (size_t)k;
+#pragma unroll
+    for (int j = 0; j < 32; j += 8) {
+        const int c = c0 + ty + j, r = r0 + tx;
+        if (r < k && c < cols) {
+            __nv_bfloat16 t[3];
+            split3(tile[tx][ty + j], t[0], t[1], t[2]);
+            __nv_bfloat16* o = out + (size_t)c * kq + r;
+#pragma unroll
+            for (int s = 0; s < 6; s++) o[(size_t)s * k] = t[kTseg[s]];
+        }
+    }
+}
+
 }  // namespace
+
+// The BF16x6 operands of a block step: aq: rows_l x 6k, bq: cols_t x 6k.
+int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
+                uint8_t* bq, cudaStream_t st) {
+    if (rows_l <= 0 || cols_t <= 0) return LP_OK;
+    const size_t total = (size_t)rows_l * k;
+    const int grid = (int)((total + 255) / 256 < 4736 ? (total + 255) / 256 : 4736);
+    k_split_rows<<<grid, 256, 0, st>>>(L, ldl, reinterpret_cast<__nv_bfloat16*>(aq), rows_l, k);
+    const dim3 tgrid((cols_t + 31) / 32, (k + 31) / 32);
+    k_split_trans<<<tgrid, 256, 0, st>>>(T, ldt, reinterpret_cast<__nv_bfloat16*>(bq), k, cols_t);
+    count_launch(2);
+    LP_CUDA(cudaGetLastError());
+    return LP_OK;
+}
 
 // Rounds the panel of a block step to the tensor-core operand type.
 // L: rows_l x k (ld ldl), T: k x cols_t (ld ldt); aq: rows_l x k, bq:
@@ -140,20 +214,23 @@ int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l,
 // One trailing (sub)update of the mixed schedule: rows [m_off, m_off+m) and
 // columns [n_off, n_off+n) of the trailing matrix at c11.
 static int mixed_update(lp_ctx* c, float* c11, int lda, const uint8_t* aq, const uint8_t* bq, int rest, int m_off,
-                        int n_off, int m, int n, int bs, bool fp8, const float* sc, int nblk, cudaStream_t st) {
+                        int n_off, int m, int n, int kq, bool fp8, const float* sc, int nblk, cudaStream_t st) {
     const float* scale_a = fp8 ? sc + nblk : nullptr;
     const float* scale_b = fp8 ? sc + 4 * nblk : nullptr;
-    return launch_umma_update(c11, lda, aq, rest, bq, rest, m_off, n_off, m, n, bs, fp8, scale_a, scale_b,
+    return launch_umma_update(c11, lda, aq, rest, bq, rest, m_off, n_off, m, n, kq, fp8, scale_a, scale_b,
                               static_cast<int*>(c->err.ptr), st);
 }
 
 int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st) {
     const bool fp8 = precision == LP_FP8_IR;
+    const bool x6 = precision == LP_F32_BF16X6;
     if (bs < 128 || bs % 128 != 0) return fail(LP_E_INVALID, "mixed precision needs a block size >= 128");
     const size_t esz = fp8 ? 1 : 2;
-    const size_t pan = (size_t)bs * n;
+    const int kq = x6 ? 6 * bs : bs;  // K of the tensor-core update
+    const size_t pan = (size_t)kq * n;      // one tensor-core operand
+    const size_t pan_f = (size_t)bs * n;    // one FP32 panel
     const int nblk = (n + 511) / 512;
-    LP_CHECK(c->lt.ensure(2 * sizeof(float) * pan));
+    LP_CHECK(c->lt.ensure(2 * sizeof(float) * pan_f));
     if (bs > 128) {
         LP_CHECK(c->lti.ensure(2 * sizeof(float) * (size_t)128 * bs));
         LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
@@ -162,7 +239,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)nblk));
     LP_CHECK(c->err.ensure(sizeof(int)));
     LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
-    float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + pan};
+    float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + pan_f};
     uint8_t* q = static_cast<uint8_t*>(c->q.ptr);
     uint8_t* aqb[2] = {q, q + 2 * esz * pan};
     uint8_t* bqb[2] = {q + esz * pan, q + 3 * esz * pan};
@@ -176,8 +253,11 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
         if (rest <= 0) return LP_OK;
         float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
         const int e = prof_begin(c, s);
-        LP_CHECK(quantize_panel(d + (size_t)bs * lda, lda, d + bs, lda, rest, rest, bs, fp8, aqb[K & 1],
-                                bqb[K & 1], scb[K & 1], nblk, s));
+        if (x6)
+            LP_CHECK(split_panel(d + (size_t)bs * lda, lda, d + bs, lda, rest, rest, bs, aqb[K & 1], bqb[K & 1], s));
+        else
+            LP_CHECK(quantize_panel(d + (size_t)bs * lda, lda, d + bs, lda, rest, rest, bs, fp8, aqb[K & 1],
+                                    bqb[K & 1], scb[K & 1], nblk, s));
         return prof_end(c, s, LP_STAGE_OTHER, e, 0.0, 2.0 * 4.0 * b * rest + 2.0 * esz * b * rest);
     };
 
@@ -190,8 +270,8 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
         const uint8_t* bq = bqb[K & 1];
         const float* sc = scb[K & 1];
         int e = prof_begin(c, st);
-        LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, 0, 0, bs, rest, bs, fp8, sc, nblk, st));
-        if (rest > bs) LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, 0, rest - bs, bs, bs, fp8, sc, nblk, st));
+        LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, 0, 0, bs, rest, kq, fp8, sc, nblk, st));
+        if (rest > bs) LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, 0, rest - bs, bs, kq, fp8, sc, nblk, st));
         LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, 2.0 * b * r * b + 2.0 * (r - b) * b * b,
                           8.0 * (b * r + (r - b) * b)));
         LP_CUDA(cudaEventRecord(c->ev_fork, st));
@@ -201,7 +281,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
         if (rest > bs) {
             const double r2 = rest - bs;
             e = prof_begin(c, st);
-            LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, bs, rest - bs, rest - bs, bs, fp8, sc, nblk, st));
+            LP_CHECK(mixed_update(c, c11, lda, aq, bq, rest, bs, bs, rest - bs, rest - bs, kq, fp8, sc, nblk, st));
             LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, 2.0 * r2 * r2 * b, 8.0 * r2 * r2));
         }
         LP_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));

@@ -521,7 +521,7 @@ int lp_gefa_prec_dev(lp_ctx* c, int precision, float* dA, int n, int lda, int bs
     if (c == nullptr) return fail(LP_E_INVALID, "lp_gefa_prec_dev: null context");
     LP_CHECK(validate_matrix(dA, n, lda, bs, "lp_gefa_prec_dev"));
     if (!aligned16(dA)) return fail(LP_E_INVALID, "lp_gefa_prec_dev: matrix must be 16-byte aligned");
-    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR)
+    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR && precision != LP_F32_BF16X6)
         return fail(LP_E_INVALID, "lp_gefa_prec_dev: unknown precision");
     LP_CUDA(cudaSetDevice(c->device));
     if (precision == LP_F32) return gefa_f32(c, dA, n, lda, bs, c->stream);
@@ -619,7 +619,7 @@ int lp_solve_host(lp_ctx* c, int precision, int n, int bs, float* A, int lda, co
     if (c == nullptr || b64 == nullptr || x == nullptr) return fail(LP_E_INVALID, "lp_solve_host: null argument");
     LP_CHECK(validate_matrix(A, n, lda, bs, "lp_solve_host"));
     if (nrhs <= 0) return fail(LP_E_INVALID, "lp_solve_host: nrhs must be positive");
-    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR)
+    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR && precision != LP_F32_BF16X6)
         return fail(LP_E_INVALID, "lp_solve_host: unknown precision");
     LP_CUDA(cudaSetDevice(c->device));
     return solve_host_impl(c, precision, n, bs, A, lda, b64, nrhs, x, max_iters, t);

@@ -30,6 +30,9 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
 int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st);
 int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
                    uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st);
+// BF16x6 operands (exact three-term split, six K-segments) of a block step.
+int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
+                uint8_t* bq, cudaStream_t st);
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
                        int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
                        cudaStream_t st);

@@ -25,8 +25,8 @@ LP_E_STATE = -6
 LP_E_BUDGET = -7
 LP_E_NODEVICE = -8
 
-LP_F32, LP_BF16_IR, LP_FP8_IR = 0, 1, 2
-PRECISIONS = {"f32": LP_F32, "bf16": LP_BF16_IR, "fp8": LP_FP8_IR}
+LP_F32, LP_BF16_IR, LP_FP8_IR, LP_F32_BF16X6 = 0, 1, 2, 3
+PRECISIONS = {"f32": LP_F32, "bf16": LP_BF16_IR, "fp8": LP_FP8_IR, "f32_bf16x6": LP_F32_BF16X6}
 
 _F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _F64P = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")

@@ -48,7 +48,13 @@ extern "C" {
  * diagonal-block LU and the triangular updates stay FP32; the solve is
  * refined in FP64 (residual and update) until the HPL scaled residual is
  * at most 16. */
-typedef enum { LP_F32 = 0, LP_BF16_IR = 1, LP_FP8_IR = 2 } lp_precision;
+typedef enum { LP_F32 = 0, LP_BF16_IR = 1, LP_FP8_IR = 2, LP_F32_BF16X6 = 3 } lp_precision;
+/* LP_F32_BF16X6 (no counterpart in the reference, which computes in FP32):
+ * the FP32 trailing update emulated on the BF16 tensor cores.  Every FP32
+ * operand is split exactly into three BF16 terms (x = x1 + x2 + x3) and the
+ * six cross products whose weight is at least 2^-16 of x1*t1 are accumulated
+ * in FP32; the dropped terms are below the FP32 rounding of each product, so
+ * the factors have FP32 accuracy and need no refinement (max_iters may be 0). */
 
 typedef struct lp_ctx lp_ctx;
 

@@ -90,7 +90,8 @@ def test_left_update_bitexact(ctx, dev, bs, nrows):
     assert np.array_equal(bits(dev.get(dLt)[:, :nrows]), bits(np.ascontiguousarray(want.T)))
 
 
-@pytest.mark.parametrize("m,n,bs", [(16, 16, 16), (128, 128, 128), (48, 80, 32), (300, 260, 64), (512, 1024, 512)])
+@pytest.mark.parametrize("m,n,bs", [(16, 16, 16), (128, 128, 128), (48, 80, 32), (300, 260, 64), (512, 1024, 512),
+                                    (1024, 1536, 512), (1100, 1300, 128), (2048, 520, 16)])
 def test_inner_update(ctx, dev, m, n, bs):
     rng = np.random.default_rng(m * n + bs)
     C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
