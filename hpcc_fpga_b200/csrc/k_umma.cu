@@ -5,12 +5,13 @@
 // Aq: the left panel rounded to BF16 (or FP8 E4M3), m x k, k contiguous;
 // Bq: the top panel rounded the same way and stored transposed, n x k.
 // Both are K-major operands.  Persistent, warp-specialized: one CTA per SM
-// walks 128 x 128 C tiles (row-block-major, so neighbouring CTAs share the A
-// tile in L2).
+// walks 128 x TN C tiles (in groups of 16 tile rows, so that the CTAs in
+// flight share their A and B tiles in L2); TN = 256 where the column range allows it (half the operand
+// bytes per flop of TN = 128, which matters once K is long), else 128.
 //   warp 0      TMA producer: A and B tiles (128-byte swizzle) into a
 //               STAGES-deep shared-memory ring;
 //   warp 1      one elected thread issues tcgen05.mma (kind::f16 for BF16,
-//               kind::f8f6f4 for E4M3) into one of TWO 128-column FP32
+//               kind::f8f6f4 for E4M3) into one of TWO TN-column FP32
 //               accumulators in tensor memory, alternating by tile;
 //   warps 2-9   epilogue: while the next tile's MMAs run, read the finished
 //               accumulator with tcgen05.ld (warp w reads TMEM lanes
@@ -34,17 +35,22 @@ namespace lp {
 namespace {
 
 constexpr int UM = 128;            // tile rows (TMEM lanes)
-constexpr int UN = 128;            // tile columns (TMEM columns)
+constexpr int UN = 128;            // narrow tile columns (TMEM columns); the wide tile has 2 UN
 constexpr int UKB = 128;           // bytes of k per stage row (one 128-byte swizzle row)
-constexpr int USTAGES = 4;
 constexpr int UEPI = 8;            // epilogue warps
 constexpr int UT = 32 * (2 + UEPI);
 constexpr int kTileBytesA = UM * UKB;
-constexpr int kTileBytesB = UN * UKB;
-constexpr int kStageBytes = kTileBytesA + kTileBytesB;
 constexpr int kScratchFloats = 32 * 33;  // per epilogue warp: one 32 x 32 block, padded
-constexpr size_t kUmmaSmem = (size_t)USTAGES * kStageBytes + sizeof(float) * UEPI * kScratchFloats +
-                             1024 /*align slack*/ + 256 /*barriers*/;
+// Ring depth: 4 stages of 32 KB for TN = 128, 3 of 48 KB for TN = 256.
+template <int TN>
+__host__ __device__ constexpr int stages() { return TN == 128 ? 4 : 3; }
+template <int TN>
+__host__ __device__ constexpr int stage_bytes() { return kTileBytesA + TN * UKB; }
+template <int TN>
+constexpr size_t umma_smem() {
+    return (size_t)stages<TN>() * stage_bytes<TN>() + sizeof(float) * UEPI * kScratchFloats + 1024 /*align slack*/ +
+           256 /*barriers*/;
+}
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;
 
@@ -141,19 +147,38 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 // Instruction descriptor: FP32 accumulate (c_format 1), A/B K-major,
 // N >> 3 at bits 17-22, M >> 4 at bits 24-28; a/b format 1 = BF16 for
 // kind::f16, 0 = E4M3 for kind::f8f6f4.
-template <bool FP8>
+// Tile t -> its C origin.  Tiles go down groups of kGroupRows tile rows
+// column by column, so the ~140 tiles in flight at once span 16 row blocks
+// of A and about 9 column blocks of B, which stay in L2; a plain row-major
+// order would stream all of B from HBM once per tile row.
+constexpr int kGroupRows = 16;
+__device__ __forceinline__ void tile_origin(int t, int tiles_n, int tiles, int m_off, int n_off, int tn, int* m0,
+                                            int* n0) {
+    const int tiles_m = tiles / tiles_n;
+    const int group = t / (kGroupRows * tiles_n);
+    const int first = group * kGroupRows;
+    const int rows = min(kGroupRows, tiles_m - first);
+    const int local = t - first * tiles_n;
+    *m0 = m_off + (first + local % rows) * UM;
+    *n0 = n_off + (local / rows) * tn;
+}
+
+template <bool FP8, int TN>
 __host__ __device__ constexpr uint32_t idesc_value() {
-    return (1u << 4) | ((FP8 ? 0u : 1u) << 7) | ((FP8 ? 0u : 1u) << 10) | ((uint32_t)(UN >> 3) << 17) |
+    return (1u << 4) | ((FP8 ? 0u : 1u) << 7) | ((FP8 ? 0u : 1u) << 10) | ((uint32_t)(TN >> 3) << 17) |
            ((uint32_t)(UM >> 4) << 24);
 }
 
-template <bool FP8>
+template <bool FP8, int TN>
 __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ CUtensorMap map_a,
                                                        const __grid_constant__ CUtensorMap map_b,
                                                        float* __restrict__ C, int ldc, int m_off, int n_off,
                                                        int tiles_n, int tiles, int kbytes,
                                                        const float* __restrict__ scale_a,
                                                        const float* __restrict__ scale_b, int* __restrict__ err) {
+    constexpr int USTAGES = stages<TN>();
+    constexpr int kStageBytes = stage_bytes<TN>();
+    constexpr int kBlk = TN / 64;  // 32-column blocks per epilogue warp
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -187,7 +212,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     __syncwarp();
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"((uint32_t)(2 * UN)));
+                     "r"((uint32_t)(2 * TN)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     tc_fence_before();
@@ -200,7 +225,8 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
             int it = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-                const int m0 = m_off + (t / tiles_n) * UM, n0 = n_off + (t % tiles_n) * UN;
+                int m0, n0;
+                tile_origin(t, tiles_n, tiles, m_off, n_off, TN, &m0, &n0);
                 for (int kt = 0; kt < KT; kt++, it++) {
                     const int s = it % USTAGES;
                     if (!mbar_wait(&empty[s], ((it / USTAGES) & 1) ^ 1, abort_flag)) {
@@ -223,7 +249,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
         }
     } else if (warp == 1) {
         if (lane == 0) {  // MMA issuer
-            constexpr uint32_t idesc = idesc_value<FP8>();
+            constexpr uint32_t idesc = idesc_value<FP8, TN>();
             int it = 0, i = 0;
             bool ok = true;
             for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, i++) {
@@ -234,7 +260,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
                     break;
                 }
                 tc_fence_after();
-                const uint32_t acc = tmem + (uint32_t)(b * UN);
+                const uint32_t acc = tmem + (uint32_t)(b * TN);
                 for (int kt = 0; kt < KT; kt++, it++) {
                     const int s = it % USTAGES;
                     if (!mbar_wait(&full[s], (it / USTAGES) & 1, abort_flag)) {
@@ -258,14 +284,16 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     } else {  // epilogue
         const int ew = warp - 2;
         const int quarter = warp & 3;      // TMEM lanes this warp may read
-        const int half = ew >> 2;          // columns [64 half, 64 half + 64)
+        const int half = ew >> 2;          // columns [TN/2 half, TN/2 half + TN/2)
         float* scr = scratch + ew * kScratchFloats;
         int i = 0;
         for (int t = blockIdx.x; t < tiles; t += gridDim.x, i++) {
             const int b = i & 1;
-            const int m0 = m_off + (t / tiles_n) * UM, n0 = n_off + (t % tiles_n) * UN;
-            const int r0 = m0 + quarter * 32, c0 = n0 + half * 64;
-            // prefetch this warp's 32 x 64 piece of C, one coalesced row segment per load
+            int m0, n0;
+            tile_origin(t, tiles_n, tiles, m_off, n_off, TN, &m0, &n0);
+            const int r0 = m0 + quarter * 32, c0 = n0 + half * (TN / 2);
+            // prefetch the first two 32 x 32 blocks of this warp's 32 x TN/2 piece of C (one
+            // coalesced row segment per load); block b + 2 is fetched while block b + 1 is added
             float cv[2][32];
 #pragma unroll
             for (int blk = 0; blk < 2; blk++)
@@ -280,13 +308,13 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
             }
             tc_fence_after();
             const float sc = (scale_a != nullptr) ? scale_a[m0 >> 9] * scale_b[n0 >> 9] : 1.0f;
-            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * UN + half * 64);
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * TN + half * (TN / 2));
 #pragma unroll
-            for (int blk = 0; blk < 2; blk++) {
+            for (int blk = 0; blk < kBlk; blk++) {
                 uint32_t a[32];
                 tmem_ld32(taddr + 32 * blk, a);  // lane = tile row, 32 consecutive columns
                 tmem_wait_ld();
-                if (blk == 1) {
+                if (blk == kBlk - 1) {
                     // both halves of the accumulator are in registers: hand the buffer back
                     tc_fence_before();
                     __syncwarp();
@@ -297,8 +325,13 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
                 __syncwarp();
 #pragma unroll
                 for (int r = 0; r < 32; r++) {
-                    const float v = fmaf(sc, scr[r * 33 + lane], cv[blk][r]);
+                    const float v = fmaf(sc, scr[r * 33 + lane], cv[blk & 1][r]);
                     C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane] = v;
+                }
+                if (blk + 2 < kBlk) {
+#pragma unroll
+                    for (int r = 0; r < 32; r++)
+                        cv[blk & 1][r] = C[(size_t)(r0 + r) * ldc + c0 + 32 * (blk + 2) + lane];
                 }
                 __syncwarp();
             }
@@ -316,7 +349,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * UN)));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * TN)));
     }
 }
 
@@ -344,15 +377,15 @@ int encode_fn(EncodeTiledFn* out) {
 }
 
 // 2-D tensor map over a row-major (rows x kbytes-of-k) operand with 128-byte
-// swizzled boxes of (128 bytes of k) x 128 rows.
-int make_map(CUtensorMap* map, const void* base, int rows, int kelems, bool fp8) {
+// swizzled boxes of (128 bytes of k) x box_rows rows.
+int make_map(CUtensorMap* map, const void* base, int rows, int kelems, bool fp8, int box_rows) {
     EncodeTiledFn encode = nullptr;
     LP_CHECK(encode_fn(&encode));
     const CUtensorMapDataType dt = fp8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
     const int esz = fp8 ? 1 : 2;
     const cuuint64_t dims[2] = {(cuuint64_t)kelems, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)kelems * esz};
-    const cuuint32_t box[2] = {(cuuint32_t)(UKB / esz), (cuuint32_t)UM};
+    const cuuint32_t box[2] = {(cuuint32_t)(UKB / esz), (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     CUresult r = encode(map, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -364,8 +397,14 @@ int make_map(CUtensorMap* map, const void* base, int rows, int kelems, bool fp8)
 }  // namespace
 
 int umma_init_attrs() {
-    LP_CUDA(cudaFuncSetAttribute(k_umma_update<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem));
-    LP_CUDA(cudaFuncSetAttribute(k_umma_update<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUmmaSmem));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<false, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<true, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<false, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<256>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<256>()));
     return LP_OK;
 }
 
@@ -382,10 +421,13 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
         !aligned16(bq) || m_off + m > aq_rows || n_off + n > bq_rows)
         return fail(LP_E_INVALID, "umma_update: tile-aligned sizes and 16-byte aligned operands required");
     if (fp8 && (scale_a == nullptr || scale_b == nullptr)) return fail(LP_E_INVALID, "umma_update: fp8 needs scales");
+    // the wide tile where the column range is a multiple of it
+    const bool wide = n % (2 * UN) == 0 && n_off % (2 * UN) == 0;
+    const int tn = wide ? 2 * UN : UN;
     CUtensorMap ma, mb;
-    LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8));
-    LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8));
-    const int tiles_n = n / UN, tiles = tiles_n * (m / UM);
+    LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8, UM));
+    LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8, tn));
+    const int tiles_n = n / tn, tiles = tiles_n * (m / UM);
     int dev = 0, sms = 0;
     LP_CUDA(cudaGetDevice(&dev));
     LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -396,12 +438,18 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     constexpr int kPanelSMs = 8;
     const int usable = sms - kPanelSMs > 1 ? sms - kPanelSMs : 1;
     const int grid = tiles < usable ? tiles : usable;
-    if (fp8)
-        k_umma_update<true><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles, kbytes, scale_a,
-                                                         scale_b, err);
+    if (fp8 && wide)
+        k_umma_update<true, 256><<<grid, UT, umma_smem<256>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
+                                                                     kbytes, scale_a, scale_b, err);
+    else if (fp8)
+        k_umma_update<true, 128><<<grid, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
+                                                                     kbytes, scale_a, scale_b, err);
+    else if (wide)
+        k_umma_update<false, 256><<<grid, UT, umma_smem<256>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
+                                                                      kbytes, nullptr, nullptr, err);
     else
-        k_umma_update<false><<<grid, UT, kUmmaSmem, st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles, kbytes,
-                                                          nullptr, nullptr, err);
+        k_umma_update<false, 128><<<grid, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
+                                                                      kbytes, nullptr, nullptr, err);
     count_launch();
     LP_CUDA(cudaGetLastError());
     return LP_OK;
