@@ -55,8 +55,8 @@ public:
         if (torus_width <= 0 || mpi_size % torus_width != 0)
             throw std::runtime_error("MPI size not dividable by P=" + std::to_string(torus_width) + "!");
         torus_height = mpi_size / torus_width;
-        if (precision != "f32" && precision != "bf16" && precision != "fp8")
-            throw std::runtime_error("Unknown precision '" + precision + "' (f32, bf16, fp8)");
+        if (precision != "f32" && precision != "bf16" && precision != "fp8" && precision != "f32_bf16x6")
+            throw std::runtime_error("Unknown precision '" + precision + "' (f32, bf16, fp8, f32_bf16x6)");
         if (generator != "reference" && generator != "baseline")
             throw std::runtime_error("Unknown generator '" + generator + "' (reference, baseline)");
     }
@@ -156,7 +156,7 @@ inline std::map<std::string, std::vector<double>> calculate_mixed(
     const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data, int* iters,
     double* hpl_resid) {
     const auto& s = *config.programSettings;
-    const int prec = s.precision == "bf16" ? LP_BF16_IR : LP_FP8_IR;
+    const int prec = s.precision == "bf16" ? LP_BF16_IR : s.precision == "fp8" ? LP_FP8_IR : LP_F32_BF16X6;
     const int n = (int)s.matrixSize;
     std::vector<double> b64(n), x(n);
     for (int i = 0; i < n; i++) b64[i] = data.b64.empty() ? (double)data.b[i] : data.b64[i];
@@ -199,7 +199,10 @@ protected:
                              "the FPGA kernel!")
             .flag("emulation", "Use kernel arguments for emulation. This may be necessary to simulate persistent local "
                                "memory on the FPGA")
-            .value("precision", "Trailing-update precision: f32, bf16 or fp8 (bf16/fp8 refine in FP64)", "f32")
+            .value("precision",
+                   "Trailing-update precision: f32, bf16, fp8 (bf16/fp8 refine in FP64) or f32_bf16x6 (FP32 emulated "
+                   "on the BF16 tensor cores; refines only if --max-refinements > 0 and needed)",
+                   "f32")
             .value("generator", "Input generator: reference (mt19937(0), U(0,1)) or baseline (seeded, U[-0.5,0.5))",
                    "reference")
             .value("seed", "Seed of the baseline generator", "42")

@@ -106,6 +106,18 @@ def test_lp_bench_mixed_precision(tmp_path, lp, prec):
 
 
 @pytest.mark.gpu
+def test_lp_bench_fp32_emulated(tmp_path, lp):
+    """FP32 emulated on the tensor cores validates like FP32, with no refinement."""
+    out = tmp_path / "emu.json"
+    r = run(["-f", "hpl_CUDA", "-m", "8", "-b", "9", "-n", "1", "--precision", "f32_bf16x6", "--max-refinements", "0",
+             "--dump-json", str(out)])
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Validation: SUCCESS!" in r.stdout
+    j = json.loads(out.read_text())
+    assert j["errors"]["residual_norm"] < 1.0
+
+
+@pytest.mark.gpu
 def test_lp_bench_unsupported_comm_type(lp):
     r = run(["-f", "hpl_torus_PCIE.aocx", "-m", "2", "-b", "5", "--comm-type", "PCIE"])
     assert r.returncode == 1
