@@ -53,6 +53,8 @@ int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, i
 // FP64 form (lp_fp64.cu): factorization and substitution in double.
 int gefa_f64(lp_ctx* c, double* a, int n, int lda, int bs, cudaStream_t st);
 int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st);
+// The same substitution in FP64 arithmetic on FP32 factors (widened exactly).
+int gesl_f64_on_f32(lp_ctx* c, const float* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st);
 // Partial pivoting (k_pivot.cu): kernels of the blocked LINPACK-convention LU.
 int piv_init_attrs();
 size_t piv_sync_bytes();
@@ -65,6 +67,9 @@ int launch_piv_desc(const int* ipvt, int n, int pb, int* desc, cudaStream_t st);
 int launch_piv_convert(float* a, int lda, int n, int pb, const int* ipvt, bool to_reference, cudaStream_t st);
 int launch_piv_gesl(const float* a, int lda, int n, int pb, const int* desc, float* b, int ldb, int nrhs, float* w,
                     unsigned char* sync, int sms, cudaStream_t st);
+// Restarted left-preconditioned GMRES in FP64 (lp_gmres.cu).
+int gmres_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b, double* x, int restart,
+               int max_it, double tol, int* steps_out, double* resid_out, cudaStream_t st);
 // Waits for the work queued on st so far without spinning a CPU core.
 int wait_stream(lp_ctx* c, cudaStream_t st);
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
@@ -101,6 +106,9 @@ struct lp_ctx {
     lp::Workspace dnorm;                      // refinement norms (device)
     unsigned long long* hnorm = nullptr;      // their pinned host copy
     size_t hnorm_cap = 0;
+    lp::Workspace gmw;                        // GMRES: Krylov basis and work vectors
+    double* hgm = nullptr;                    // GMRES: pinned Hessenberg column
+    size_t hgm_cap = 0;
     lp::Workspace f64a, f64b, f64lt, f64w;  // FP64: host-entry matrix and rhs, transposed left panel, solve vectors
     lp::Workspace psync, pat, pdesc, pw, pipvt;  // pivoting: barrier + exchange area, transposed U12,
                                                  // interchange permutations, solve vectors, ipvt
@@ -121,7 +129,7 @@ struct lp_ctx {
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
         lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
-                                &dnorm, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
+                                &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
         bgraph = nullptr;
@@ -132,5 +140,8 @@ struct lp_ctx {
         if (hnorm != nullptr) cudaFreeHost(hnorm);
         hnorm = nullptr;
         hnorm_cap = 0;
+        if (hgm != nullptr) cudaFreeHost(hgm);
+        hgm = nullptr;
+        hgm_cap = 0;
     }
 };

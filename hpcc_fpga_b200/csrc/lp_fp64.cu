@@ -22,7 +22,9 @@ constexpr int GT = 256;      // threads per CTA; one unknown per thread in the u
 constexpr int RMAX = 16;     // right-hand sides per pass
 
 // The kb x kb diagonal block into shared memory, every copy in flight before
-// the wait; entries outside it are zero.
+// the wait; entries outside it are zero.  FP32 factors (the substitution in
+// FP64 arithmetic on FP32 factors, used by the GMRES refinement) are widened
+// exactly as they are read.
 __device__ __forceinline__ void stage_block(double (*dg)[SB + 1], const double* __restrict__ a, int lda, int k0,
                                             int kb) {
     for (int idx = threadIdx.x; idx < SB * SB; idx += GT) {
@@ -34,18 +36,33 @@ __device__ __forceinline__ void stage_block(double (*dg)[SB + 1], const double* 
     }
     cp_async_wait_all();
 }
+__device__ __forceinline__ void stage_block(double (*dg)[SB + 1], const float* __restrict__ a, int lda, int k0,
+                                            int kb) {
+    float v[SB * SB / GT];
+#pragma unroll
+    for (int q = 0; q < SB * SB / GT; q++) {  // all loads in flight before the first store
+        const int idx = threadIdx.x + q * GT, r = idx / SB, c = idx - r * SB;
+        v[q] = (r < kb && c < kb) ? __ldg(a + (size_t)(k0 + r) * lda + k0 + c) : 0.0f;
+    }
+#pragma unroll
+    for (int q = 0; q < SB * SB / GT; q++) {
+        const int idx = threadIdx.x + q * GT, r = idx / SB, c = idx - r * SB;
+        dg[r][c] = (double)v[q];
+    }
+}
 
 // acc[r] = sum_{k < kb} coef[r][k] * S[k0 + k][c]: the block's column c, read
 // 16 rows at a time with all 16 loads in flight before they are used.
-__device__ __forceinline__ void block_gemv(const double* __restrict__ a, int lda, int k0, int kb, int c,
+template <typename FT>
+__device__ __forceinline__ void block_gemv(const FT* __restrict__ a, int lda, int k0, int kb, int c,
                                            const double (*coef)[SB], int nrhs, double (&acc)[RMAX]) {
 #pragma unroll
     for (int r = 0; r < RMAX; r++) acc[r] = 0.0;
-    const double* col = a + (size_t)k0 * lda + c;
+    const FT* col = a + (size_t)k0 * lda + c;
     for (int kc = 0; kc < kb; kc += 16) {
         double v[16];
 #pragma unroll
-        for (int j = 0; j < 16; j++) v[j] = kc + j < kb ? __ldg(col + (size_t)(kc + j) * lda) : 0.0;
+        for (int j = 0; j < 16; j++) v[j] = kc + j < kb ? (double)__ldg(col + (size_t)(kc + j) * lda) : 0.0;
 #pragma unroll
         for (int r = 0; r < RMAX; r++)
             if (r < nrhs)
@@ -57,7 +74,8 @@ __device__ __forceinline__ void block_gemv(const double* __restrict__ a, int lda
 
 // forward: y_i += y_k S[k][i] (i > k).  w1: accumulating values (all
 // unknowns), w2: solved values of the block.
-__global__ void __launch_bounds__(GT) k_gesl64_fwd(const double* __restrict__ a, int lda, int n, double* w1,
+template <typename FT>
+__global__ void __launch_bounds__(GT) k_gesl64_fwd(const FT* __restrict__ a, int lda, int n, double* w1,
                                                    double* w2, int ldw, int nrhs, int k0) {
     __shared__ double dg[SB][SB + 1];
     __shared__ double ys[RMAX][SB];
@@ -92,7 +110,8 @@ __global__ void __launch_bounds__(GT) k_gesl64_fwd(const double* __restrict__ a,
 
 // backward: s = y_k S[k][k]; x_k = -s; y_i += s S[k][i] (i < k).  w2: values
 // (updated in place for the unknowns before the block), out: solutions.
-__global__ void __launch_bounds__(GT) k_gesl64_bwd(const double* __restrict__ a, int lda, int n, double* w2, int ldw,
+template <typename FT>
+__global__ void __launch_bounds__(GT) k_gesl64_bwd(const FT* __restrict__ a, int lda, int n, double* w2, int ldw,
                                                    double* out, int ldo, int nrhs, int k0) {
     __shared__ double dg[SB][SB + 1];
     __shared__ double ss[RMAX][SB];
@@ -173,7 +192,8 @@ int gefa_f64(lp_ctx* c, double* a, int n, int lda, int bs, cudaStream_t st) {
     return LP_OK;
 }
 
-int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st) {
+template <typename FT>
+static int gesl64_any(lp_ctx* c, const FT* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st) {
     const int g0 = nrhs < RMAX ? nrhs : RMAX;
     LP_CHECK(c->f64w.ensure(sizeof(double) * 2 * (size_t)n * g0));
     double* w1 = static_cast<double*>(c->f64w.ptr);
@@ -188,18 +208,27 @@ int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, in
         for (int K = 0; K < nblk; K++) {
             const int k0 = K * SB, rest = n - k0 - std::min(SB, n - k0);
             const int grid = rest > 0 ? (rest + GT - 1) / GT : 1;
-            k_gesl64_fwd<<<grid, GT, 0, st>>>(a, lda, n, w1, w2, n, g, k0);
+            k_gesl64_fwd<FT><<<grid, GT, 0, st>>>(a, lda, n, w1, w2, n, g, k0);
             count_launch();
         }
         for (int K = nblk - 1; K >= 0; K--) {
             const int k0 = K * SB;
             const int grid = k0 > 0 ? (k0 + GT - 1) / GT : 1;
-            k_gesl64_bwd<<<grid, GT, 0, st>>>(a, lda, n, w2, n, bb, ldb, g, k0);
+            k_gesl64_bwd<FT><<<grid, GT, 0, st>>>(a, lda, n, w2, n, bb, ldb, g, k0);
             count_launch();
         }
         LP_CUDA(cudaGetLastError());
     }
-    return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * n * n * nrhs, 8.0 * n * n * ((nrhs + RMAX - 1) / RMAX));
+    return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * n * n * nrhs,
+                    (double)sizeof(FT) * n * n * ((nrhs + RMAX - 1) / RMAX));
+}
+
+int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st) {
+    return gesl64_any(c, a, n, lda, b, nrhs, ldb, st);
+}
+
+int gesl_f64_on_f32(lp_ctx* c, const float* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st) {
+    return gesl64_any(c, a, n, lda, b, nrhs, ldb, st);
 }
 
 }  // namespace lp

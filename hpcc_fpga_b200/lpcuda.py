@@ -169,6 +169,7 @@ def lib() -> ctypes.CDLL:
     L.lp_gesl_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
     L.lp_gesl_dev_noalloc.argtypes = [_VP, _I, _I, _VP, _I, _I, _VP]
     L.lp_calculate.argtypes = [_VP, _I, _I, _I, _I, _F32P, _F32P, _F64P, _F64P]
+    L.lp_gmres_dev.argtypes = [_VP, _VP, _I, _VP, _I, _VP, _VP, _I, _I, ctypes.c_double, ctypes.POINTER(LpTiming)]
     L.lp_gefa_f64_dev.argtypes = [_VP, _VP, _I, _I, _I]
     L.lp_gesl_f64_dev.argtypes = [_VP, _VP, _I, _I, _VP, _I, _I]
     L.lp_calculate_f64.argtypes = [_VP, _I, _I, _I, _I, _F64P, _F64P, _F64P, _F64P]
@@ -336,6 +337,14 @@ class Context:
 
     def gesl(self, dLU: int, n: int, lda: int, dB: int, nrhs: int = 1, ldb: int | None = None) -> None:
         check(lib().lp_gesl_dev(self._h, dLU, n, lda, dB, nrhs, n if ldb is None else ldb), "lp_gesl_dev")
+
+    def gmres(self, dA0: int, lda: int, dLU: int, n: int, dB64: int, dX: int, restart: int = 50, max_it: int = 1,
+              tol: float = 1e-8) -> dict:
+        """gmres_ref on the device: dX = initial guess in, solution out."""
+        t = LpTiming()
+        check(lib().lp_gmres_dev(self._h, dA0, lda, dLU, n, dB64, dX, restart, max_it, tol, ctypes.byref(t)),
+              "lp_gmres_dev")
+        return t.as_dict()
 
     # ---- FP64 (the reference's double build) ----------------------------------
     def gefa_f64(self, dA: int, n: int, lda: int, bs: int = 128) -> None:

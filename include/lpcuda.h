@@ -179,6 +179,17 @@ int lp_gefa_prec_dev(lp_ctx* ctx, int precision, float* dA, int n, int lda, int 
  * doubles.  t (optional) receives ir_s, ir_iters and hpl_resid. */
 int lp_refine_dev(lp_ctx* ctx, const float* dA0, int lda, const float* dLU, int n, const double* dB64, double* dX,
                   int nrhs, int max_iters, lp_timing* t);
+/* GMRES-based refinement: the reference's gmres_ref
+ * (LINPACK/src/host/gmres.c:53-232) with the factors at dLU (any precision of
+ * lp_gefa_prec_dev) as left preconditioner: restarted GMRES in FP64 on
+ * LU^-1 A x = LU^-1 b, A the original FP32 matrix dA0 widened to FP64.  dX
+ * holds the initial guess on entry (gmres_ref's x) and the solution on return;
+ * stops when the preconditioned residual estimate is <= tol * |b| and the HPL
+ * scaled residual (eps = DBL_EPSILON/2) is <= 16, or after max_it restart
+ * cycles of `restart` steps.  t (optional): ir_s, ir_iters = Arnoldi steps,
+ * hpl_resid.  One right-hand side. */
+int lp_gmres_dev(lp_ctx* ctx, const float* dA0, int lda, const float* dLU, int n, const double* dB64, double* dX,
+                 int restart, int max_it, double tol, lp_timing* t);
 /* Forward + back substitution with the encoded factors for nrhs right-hand
  * sides stored as rows of dB (dB[r*ldb + i]); the solutions overwrite dB.
  * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229). */
