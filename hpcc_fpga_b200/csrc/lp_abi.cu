@@ -229,7 +229,24 @@ int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cu
 // Lt is double-buffered so panel K+1 never overwrites the operand U_b reads.
 // top and left give the reference recurrences' values up to rounding
 // (blocked); the exact recurrences are lp_top_update_dev/lp_left_update_dev.
-int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
+// The final bands of block step K (its block row right of and including the
+// diagonal block, its block column below it) to the sink's host mirror.
+static int sink_bands(const FactorSink* s, const float* dA, int n, int lda, int bs, int K, cudaStream_t done_on) {
+    if (s == nullptr) return LP_OK;
+    cudaEvent_t ev = (*s->events)[K];
+    LP_CUDA(cudaEventRecord(ev, done_on));
+    LP_CUDA(cudaStreamWaitEvent(s->copy, ev, 0));
+    const size_t k0 = (size_t)K * bs, pitch = sizeof(float) * (size_t)lda;
+    LP_CUDA(cudaMemcpy2DAsync(s->host + k0 * lda + k0, pitch, dA + k0 * lda + k0, pitch, sizeof(float) * (n - k0), bs,
+                              cudaMemcpyDeviceToHost, s->copy));
+    const int below = n - (int)k0 - bs;
+    if (below > 0)
+        LP_CUDA(cudaMemcpy2DAsync(s->host + (k0 + bs) * lda + k0, pitch, dA + (k0 + bs) * lda + k0, pitch,
+                                  sizeof(float) * bs, below, cudaMemcpyDeviceToHost, s->copy));
+    return LP_OK;
+}
+
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, const FactorSink* sink) {
     const size_t pan = sizeof(float) * (size_t)bs * n;
     LP_CHECK(c->lt.ensure(2 * pan));
     if (bs > 128) {
@@ -240,6 +257,7 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
     const int nb = n / bs;
     const double b = bs;
     LP_CHECK(panel_f32(c, dA, n, lda, bs, 0, ltbuf[0], st));
+    LP_CHECK(sink_bands(sink, dA, n, lda, bs, 0, st));
     for (int K = 0; K + 1 < nb; K++) {
         const int rest = n - (K + 1) * bs;
         const double r = rest;
@@ -256,6 +274,7 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
         LP_CUDA(cudaEventRecord(c->ev_fork, st));
         LP_CUDA(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
         LP_CHECK(panel_f32(c, dA, n, lda, bs, K + 1, ltbuf[(K + 1) & 1], c->aux));
+        LP_CHECK(sink_bands(sink, dA, n, lda, bs, K + 1, c->aux));
         LP_CUDA(cudaEventRecord(c->ev_join, c->aux));
         if (rest > bs) {
             const double r2 = rest - bs;
@@ -378,6 +397,7 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c->stream != nullptr) cudaStreamSynchronize(c->stream);
     if (c->aux != nullptr) cudaStreamSynchronize(c->aux);
     if (c->aux2 != nullptr) cudaStreamSynchronize(c->aux2);
+    if (c->copy != nullptr) cudaStreamSynchronize(c->copy);
     c->release_all();
     for (int i = 0; i < 8; i++)
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
@@ -386,6 +406,7 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c->ev_side != nullptr) cudaEventDestroy(c->ev_side);
     if (c->ev_side_done != nullptr) cudaEventDestroy(c->ev_side_done);
     if (c->aux2 != nullptr) cudaStreamDestroy(c->aux2);
+    if (c->copy != nullptr) cudaStreamDestroy(c->copy);
     if (c->ev_block != nullptr) cudaEventDestroy(c->ev_block);
     if (c->aux != nullptr) cudaStreamDestroy(c->aux);
     if (c->stream != nullptr) cudaStreamDestroy(c->stream);
@@ -596,22 +617,49 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
     float* dA = static_cast<float*>(c->dA.ptr);
     float* dB = static_cast<float*>(c->dB.ptr);
     cudaStream_t st = c->stream;
-    for (int rep = 0; rep < repetitions; rep++) {
+    // Page-locked A: the last repetition's factors go back to the host band by
+    // band on a copy stream while the later block steps run (execution_pcie.hpp
+    // copies them after the loop, :695-696).  Pageable A: one copy at the end.
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, A) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();  // an unregistered pointer may leave an error behind
+    std::vector<cudaEvent_t> evs;
+    FactorSink sink;
+    if (pinned) {
+        if (c->copy == nullptr) LP_CUDA(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+        evs.resize(n / bs, nullptr);
+        for (auto& e : evs) LP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        sink.host = A;
+        sink.copy = c->copy;
+        sink.events = &evs;
+    }
+    int status = LP_OK;
+    for (int rep = 0; rep < repetitions && status == LP_OK; rep++) {
+        const bool last = rep + 1 == repetitions;
         LP_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, st));
         LP_CUDA(cudaMemcpyAsync(dB, b, sizeof(float) * n, cudaMemcpyHostToDevice, st));
         LP_CUDA(cudaEventRecord(c->ev[0], st));
-        LP_CHECK(gefa_f32(c, dA, n, lda, bs, st));
+        status = gefa_f32(c, dA, n, lda, bs, st, pinned && last ? &sink : nullptr);
+        if (status != LP_OK) break;
         LP_CUDA(cudaEventRecord(c->ev[1], st));
-        LP_CHECK(gesl_f32(c, dA, n, lda, dB, 1, n, st));
+        status = gesl_f32(c, dA, n, lda, dB, 1, n, st);
+        if (status != LP_OK) break;
         LP_CUDA(cudaEventRecord(c->ev[2], st));
         LP_CUDA(cudaStreamSynchronize(st));
         gefa_times[rep] = elapsed_s(c->ev[0], c->ev[1]);
         gesl_times[rep] = elapsed_s(c->ev[1], c->ev[2]);
     }
-    LP_CUDA(cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, st));
-    LP_CUDA(cudaMemcpyAsync(b, dB, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
-    LP_CUDA(cudaStreamSynchronize(st));
-    return LP_OK;
+    if (status == LP_OK) {
+        if (!pinned) LP_CUDA(cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, st));
+        LP_CUDA(cudaMemcpyAsync(b, dB, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
+        LP_CUDA(cudaStreamSynchronize(st));
+    }
+    if (pinned) {
+        cudaStreamSynchronize(c->copy);
+        for (auto e : evs)
+            if (e != nullptr) cudaEventDestroy(e);
+    }
+    return status;
 }
 
 int lp_solve_host(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,

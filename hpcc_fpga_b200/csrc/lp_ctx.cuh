@@ -24,7 +24,15 @@ struct Workspace {
 };
 
 int validate_matrix(const void* a, int n, int lda, int bs, const char* who);
-int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st);
+// Optional destination of the factors while they are computed: after each
+// block step's panel its final row and column bands are copied to host (a
+// pinned mirror of dA, leading dimension lda) on the copy stream.
+struct FactorSink {
+    float* host = nullptr;
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t>* events = nullptr;  // one per block step
+};
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, const FactorSink* sink = nullptr);
 int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st);
 // Panel work of block step K (lu, top, left; Lt into lt), on stream st.
 int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st);
@@ -90,6 +98,7 @@ struct lp_ctx {
     cudaStream_t aux = nullptr;               // second (high-priority) stream for concurrent panel work
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t aux2 = nullptr;              // third stream: the left update runs here beside the top update
+    cudaStream_t copy = nullptr;              // device-to-host copies of finished factor bands (lp_calculate)
     cudaEvent_t ev_side = nullptr, ev_side_done = nullptr;
     cudaEvent_t ev_block = nullptr;           // blocking-sync event: waits yield the CPU instead of spinning
     cudaEvent_t ev[8] = {nullptr};

@@ -35,6 +35,24 @@ def test_calculate_reference_inputs(ctx, bs, blocks):
     assert np.abs(b_dev - 1.0).max() <= 4 * max(np.abs(x_ref - 1.0).max(), n * FLT_EPS)
 
 
+@pytest.mark.parametrize("n,bs,reps", [(1024, 128, 1), (2048, 512, 2)])
+def test_calculate_pinned_overlapped_copy(ctx, lp, n, bs, reps):
+    """Page-locked A: the factors return band by band while later block steps
+    run; the result equals the pageable path's exactly."""
+    A, b, _, _ = oracle.gen_reference(n)
+    A1, b1 = A.copy(), b.copy()
+    ctx.calculate(A1, b1, bs, repetitions=reps)
+    pa, pb = lp.Pinned((n, n)), lp.Pinned((n,))
+    try:
+        pa.array[:] = A
+        pb.array[:] = b
+        ctx.calculate(pa.array, pb.array, bs, repetitions=reps)
+        assert np.array_equal(pa.array, A1) and np.array_equal(pb.array, b1)
+    finally:
+        pa.free()
+        pb.free()
+
+
 def test_calculate_repetitions_restart_from_original(ctx):
     n, bs = 256, 64
     A, b, _, _ = oracle.gen_reference(n)
