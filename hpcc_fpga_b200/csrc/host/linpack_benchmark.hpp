@@ -55,8 +55,9 @@ public:
         if (torus_width <= 0 || mpi_size % torus_width != 0)
             throw std::runtime_error("MPI size not dividable by P=" + std::to_string(torus_width) + "!");
         torus_height = mpi_size / torus_width;
-        if (precision != "f32" && precision != "bf16" && precision != "fp8" && precision != "f32_bf16x6")
-            throw std::runtime_error("Unknown precision '" + precision + "' (f32, bf16, fp8, f32_bf16x6)");
+        if (precision != "f32" && precision != "bf16" && precision != "fp8" && precision != "f32_bf16x6" &&
+            precision != "f64")
+            throw std::runtime_error("Unknown precision '" + precision + "' (f32, bf16, fp8, f32_bf16x6, f64)");
         if (generator != "reference" && generator != "baseline")
             throw std::runtime_error("Unknown generator '" + generator + "' (reference, baseline)");
     }
@@ -67,7 +68,7 @@ public:
         map["Block Size"] = std::to_string(blockSize);
         map["Emulate"] = isEmulationKernel ? "Yes" : "No";
         map["Diagonally Dominant"] = isDiagonallyDominant ? "Yes" : "No";
-        map["Data Type"] = "float";
+        map["Data Type"] = precision == "f64" ? "double" : "float";
         map["FPGA Torus"] = "P=" + std::to_string(torus_width) + ", Q=" + std::to_string(torus_height);
         map["Precision"] = precision;
         map["Generator"] = generator;
@@ -83,6 +84,13 @@ public:
     float* b = nullptr;
     int* ipvt = nullptr;
     std::vector<double> b64;  // FP64 right-hand side of the seeded generator (addition)
+    double* A64 = nullptr;    // the double build's matrix and right-hand side (--precision f64)
+    double* bd = nullptr;
+    double norma64 = 0.0, normb64 = 0.0;
+    void use_f64() {
+        A64 = static_cast<double*>(alloc(sizeof(double) * matrix_width * matrix_height));
+        bd = static_cast<double*>(alloc(sizeof(double) * matrix_width));
+    }
     size_t matrix_width, matrix_height;
     float norma = 0.0f, normb = 0.0f;
 
@@ -95,6 +103,8 @@ public:
         release(A);
         release(b);
         release(ipvt);
+        if (A64 != nullptr) release(A64);
+        if (bd != nullptr) release(bd);
     }
     LinpackData(const LinpackData&) = delete;
     LinpackData& operator=(const LinpackData&) = delete;
@@ -151,6 +161,19 @@ inline std::map<std::string, std::vector<double>> calculate_pvt(
     return {{"gefa", gefa}, {"gesl", gesl}};
 }
 
+// The reference's double build (DATA_TYPE double): factors and solution in
+// double (data.A64, data.bd); FP64 block size 128 (64 for -b 6).
+inline std::map<std::string, std::vector<double>> calculate_f64(
+    const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data) {
+    const auto& s = *config.programSettings;
+    const int bs = s.blockSize >= 128 ? 128 : (int)s.blockSize;
+    std::vector<double> gefa(s.numRepetitions), gesl(s.numRepetitions);
+    check_lp(lp_calculate_f64(config.context, (int)s.matrixSize, (int)data.matrix_width, bs, (int)s.numRepetitions,
+                              data.A64, data.bd, gefa.data(), gesl.data()),
+             "lp_calculate_f64");
+    return {{"gefa", gefa}, {"gesl", gesl}};
+}
+
 // Mixed precision (addition): tensor-core trailing updates, FP64 refinement.
 inline std::map<std::string, std::vector<double>> calculate_mixed(
     const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data, int* iters,
@@ -200,8 +223,9 @@ protected:
             .flag("emulation", "Use kernel arguments for emulation. This may be necessary to simulate persistent local "
                                "memory on the FPGA")
             .value("precision",
-                   "Trailing-update precision: f32, bf16, fp8 (bf16/fp8 refine in FP64) or f32_bf16x6 (FP32 emulated "
-                   "on the BF16 tensor cores; refines only if --max-refinements > 0 and needed)",
+                   "Trailing-update precision: f32, bf16, fp8 (bf16/fp8 refine in FP64), f32_bf16x6 (FP32 emulated "
+                   "on the BF16 tensor cores; refines only if --max-refinements > 0 and needed) or f64 (the "
+                   "reference's double build: input, factors and solution in double)",
                    "f32")
             .value("generator", "Input generator: reference (mt19937(0), U(0,1)) or baseline (seeded, U[-0.5,0.5))",
                    "reference")
@@ -226,6 +250,21 @@ public:
             for (int i = 0; i < n; i++) d->normb = d->b[i] > d->normb ? d->b[i] : d->normb;
         }
         for (int i = 0; i < n; i++) d->ipvt[i] = i;
+        if (s.precision == "f64") {  // the double build's own input
+            d->use_f64();
+            if (s.generator == "reference") {
+                check_lp(lp_generate_reference_f64(d->A64, d->bd, n, s.isDiagonallyDominant ? 1 : 0, &d->norma64,
+                                                   &d->normb64),
+                         "lp_generate_reference_f64");
+            } else {
+                d->normb64 = 0.0;
+                for (size_t i = 0; i < (size_t)n * n; i++) d->A64[i] = d->A[i];
+                for (int i = 0; i < n; i++) {
+                    d->bd[i] = d->b64[i];
+                    d->normb64 = d->bd[i] > d->normb64 ? d->bd[i] : d->normb64;
+                }
+            }
+        }
         return d;
     }
 
@@ -237,6 +276,10 @@ public:
                                      "FP32 only (--precision f32)");
         switch (s.communicationType) {
             case CommunicationType::cuda:
+                if (s.precision == "f64") {
+                    this->timings = execution::cuda::calculate_f64(*executionSettings, data);
+                    break;
+                }
                 if (!s.isDiagonallyDominant)
                     this->timings = execution::cuda::calculate_pvt(*executionSettings, data);
                 else if (s.precision == "f32")
@@ -256,13 +299,14 @@ public:
     // linpack_benchmark.hpp:334-469 (DISTRIBUTED_VALIDATION, one rank)
     bool validateOutput(LinpackData& data) override {
         const unsigned n = executionSettings->programSettings->matrixSize;
+        const bool f64 = data.bd != nullptr;
         double resid = 0.0;
         for (size_t i = 0; i < data.matrix_width; i++) {
-            const double e = std::abs((double)data.b[i] - 1.0);
+            const double e = std::abs((f64 ? data.bd[i] : (double)data.b[i]) - 1.0);
             resid = resid > e ? resid : e;
         }
-        const double normx = data.normb;
-        const float eps = std::numeric_limits<float>::epsilon();
+        const double normx = f64 ? data.normb64 : data.normb;
+        const double eps = f64 ? std::numeric_limits<double>::epsilon() : std::numeric_limits<float>::epsilon();
         const double residn = resid / (static_cast<double>(n) * normx * eps);
         errors.emplace("epsilon", eps);
         errors.emplace("residual", resid);

@@ -25,6 +25,43 @@
 
 extern "C" {
 
+// The same generator as the reference's double build (HOST_DATA_TYPE double:
+// the draws are not narrowed, the sums are in double).
+int lp_generate_reference_f64(double* A, double* b, int n, int diag_dominant, double* norma_out, double* normb_out) {
+    if (A == nullptr || b == nullptr || n <= 0) return LP_E_INVALID;
+    std::mt19937 gen(0);
+    std::uniform_real_distribution<> dis(0.0, 1.0);
+    double norma = 0.0, normb = 0.0;
+    const size_t w = (size_t)n;
+    for (size_t r = 0; r < w; r++) {
+        double* row = A + r * w;
+        for (size_t c = 0; c < w; c++) {
+            const double v = dis(gen);
+            row[c] = v;
+            norma = (v > norma) ? v : norma;
+        }
+    }
+    if (diag_dominant) {
+        for (size_t r = 0; r < w; r++) {
+            double* row = A + r * w;
+            row[r] = 0.0;
+            double s = 0.0;
+            for (size_t c = 0; c < w; c++) s += row[c];
+            norma = (s > norma) ? s : norma;
+            row[r] = s;
+        }
+    }
+    for (size_t c = 0; c < w; c++) b[c] = 0.0;
+    for (size_t r = 0; r < w; r++) {
+        const double* row = A + r * w;
+        for (size_t c = 0; c < w; c++) b[c] += row[c];
+    }
+    for (size_t c = 0; c < w; c++) normb = (b[c] > normb) ? b[c] : normb;
+    if (norma_out != nullptr) *norma_out = norma;
+    if (normb_out != nullptr) *normb_out = normb;
+    return LP_OK;
+}
+
 int lp_generate_reference(float* A, float* b, int n, int diag_dominant, float* norma_out, float* normb_out) {
     if (A == nullptr || b == nullptr || n <= 0) return LP_E_INVALID;
     std::mt19937 gen(0);

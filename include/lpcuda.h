@@ -405,6 +405,9 @@ int lp_server_replay(lp_server* s, int count, const lp_request* reqs, const doub
  * uniform_real_distribution<double>(0,1) narrowed to float; diagonal =
  * storage-row sum when diag_dominant; b = storage-column sums. */
 int lp_generate_reference(float* A, float* b, int n, int diag_dominant, float* norma, float* normb);
+/* The same for the reference's double build (HOST_DATA_TYPE double: the
+ * uniform draws kept in double, sums in double). */
+int lp_generate_reference_f64(double* A, double* b, int n, int diag_dominant, double* norma, double* normb);
 /* Seeded benchmark-workload generator: mt19937(seed), entries
  * (u>>8)*2^-24 - 0.5; diagonal = sum|off-diagonal| + margin; b64 = M*ones in
  * FP64 (exact), b32 = (float)b64.  Either output pointer may be NULL. */

@@ -118,6 +118,22 @@ def test_lp_bench_fp32_emulated(tmp_path, lp):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("generator", ["reference", "baseline"])
+def test_lp_bench_double_build(tmp_path, lp, generator):
+    """--precision f64: the reference's DATA_TYPE double variant end to end,
+    validated with the double machine epsilon."""
+    out = tmp_path / "dp.json"
+    r = run(["-f", "hpl_CUDA", "-m", "8", "-b", "7", "-n", "2", "--precision", "f64", "--generator", generator,
+             "--dump-json", str(out)])
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "Validation: SUCCESS!" in r.stdout
+    j = json.loads(out.read_text())
+    assert j["settings"]["Data Type"] == "double"
+    assert j["errors"]["residual_norm"] < 1.0
+    assert abs(j["errors"]["epsilon"] - 2.220446049250313e-16) < 1e-20
+
+
+@pytest.mark.gpu
 def test_lp_bench_unsupported_comm_type(lp):
     r = run(["-f", "hpl_torus_PCIE.aocx", "-m", "2", "-b", "5", "--comm-type", "PCIE"])
     assert r.returncode == 1
