@@ -586,12 +586,8 @@ def main() -> None:
         dXr = torch.empty(n, dtype=torch.float64, device="cuda")
     r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64r.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
     del dB64r, dXr
-    t_max = elapsed
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-    value = world * args.steps * flops(n) / t_max / 1e9
+    from hpcc_fpga_b200.replicas import job_rate
+    value, t_max = job_rate(args.steps * flops(n) / 1e9, elapsed, device="cuda")
 
     # ---- roofline of the dominant kernel (the FP32 trailing update) ----
     inner = prof["inner"]
@@ -653,12 +649,8 @@ def main() -> None:
             walls.append(time.perf_counter() - t0)
         walls = walls[1:]
         e2e_err = float(np.abs(hb.astype(np.float64) - 1.0).max())
-        wt = sum(walls)
-        if world > 1:
-            t = torch.tensor([wt], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            wt = float(t.item())
-        e2e = {"value": world * args.steps * flops(n) / wt / 1e9, "unit": UNIT,
+        e2e_value, wt = job_rate(args.steps * flops(n) / 1e9, sum(walls), device="cuda")
+        e2e = {"value": e2e_value, "unit": UNIT,
                "h2d_bytes_per_step": 4 * n * n + 4 * n, "d2h_bytes_per_step": 4 * n * n + 4 * n,
                "ms_per_step": 1e3 * wt / args.steps, "max_abs_err_x": e2e_err,
                "api": "lp_calculate (C ABI, pinned host A and b)"}
