@@ -229,10 +229,13 @@ def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, steps, warm
         "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32_simt": value / f32_value,
         "max_abs_err_x": float(np.abs(x - 1.0).max()),
         "hpl_resid": {"eps_flt_half": r32 * 2.0 ** -29, "eps_dbl_half": r32},
+        # timed inside a seconds-long factorization: the sustained BF16 figure is the denominator
         "roofline": {"bound": "tensor", "kernel": "k_umma_update (inner stage, K = 6 bs)",
-                     "achieved": 6 * tf32eq if tf32eq else None, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
-                     "frac": 6 * tf32eq / pk["bf16_tflops"] if tf32eq else None,
-                     "fp32_equivalent_tflops": tf32eq, "peak_source": pk["source"],
+                     "achieved": 6 * tf32eq if tf32eq else None,
+                     "peak": pk.get("bf16_tflops_sustained", pk["bf16_tflops"]), "unit": "TFLOP/s",
+                     "frac": 6 * tf32eq / pk.get("bf16_tflops_sustained", pk["bf16_tflops"]) if tf32eq else None,
+                     "fp32_equivalent_tflops": tf32eq,
+                     "peak_source": pk["source"] + " (bf16_tflops_sustained; burst " + str(pk["bf16_tflops"]) + ")",
                      "per_unit": "6 x 2*m*n*bs BF16 flop per m x n trailing update (2*m*n*bs FP32-equivalent)"},
         "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]},
     }
