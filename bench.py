@@ -315,8 +315,8 @@ FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
 def run_fp64(ctx, lp, torch, stream, A, b64, n, steps, warmup, peak_fp64) -> dict:
     """The double build (DATA_TYPE double): the same system's FP32 entries
     widened to double, b in double (x = ones exactly); a step = restore A,
-    lp_gefa_f64_dev (bs 128) + lp_gesl_f64_dev, on device time."""
-    bs = 128
+    lp_gefa_f64_dev (bs 256) + lp_gesl_f64_dev, on device time."""
+    bs = 256
     with torch.cuda.stream(stream):
         dA0 = torch.from_numpy(A).to("cuda").double()
         db0 = torch.from_numpy(b64).to("cuda")
@@ -620,7 +620,7 @@ def main() -> None:
             pivot["roofline"]["frac"] = pivot["roofline"]["achieved"] / peak_tf
 
     fp64 = None
-    if not args.no_fp64 and n % 128 == 0:
+    if not args.no_fp64 and n % 256 == 0:
         fp64 = run_fp64(ctx, lp, torch, stream, A, b64, n, args.steps, max(1, min(args.warmup, 2)),
                         NUM_SMS * 64 * 2 * sm_mhz * 1e6 / 1e12)
 

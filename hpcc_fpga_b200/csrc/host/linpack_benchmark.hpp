@@ -162,11 +162,11 @@ inline std::map<std::string, std::vector<double>> calculate_pvt(
 }
 
 // The reference's double build (DATA_TYPE double): factors and solution in
-// double (data.A64, data.bd); FP64 block size 128 (64 for -b 6).
+// double (data.A64, data.bd); FP64 block size 256 (128 for -b 7, 64 for -b 6).
 inline std::map<std::string, std::vector<double>> calculate_f64(
     const hpcc_base::ExecutionSettings<LinpackProgramSettings>& config, LinpackData& data) {
     const auto& s = *config.programSettings;
-    const int bs = s.blockSize >= 128 ? 128 : (int)s.blockSize;
+    const int bs = s.blockSize >= 256 ? 256 : s.blockSize >= 128 ? 128 : (int)s.blockSize;
     std::vector<double> gefa(s.numRepetitions), gesl(s.numRepetitions);
     check_lp(lp_calculate_f64(config.context, (int)s.matrixSize, (int)data.matrix_width, bs, (int)s.numRepetitions,
                               data.A64, data.bd, gefa.data(), gesl.data()),

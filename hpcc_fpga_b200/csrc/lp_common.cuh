@@ -104,6 +104,7 @@ int launch_dgemm_update(double* c, int ldc, const double* lt, int ldlt, const do
                         cudaStream_t s);
 int dgemm_init_attrs();
 int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t s);
+int launch_transpose_f64(const double* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t s);
 // Forward + back substitution for nrhs rows of b (see k_gesl.cu).
 int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t s);
 size_t gesl_work_floats(int n, int nrhs);

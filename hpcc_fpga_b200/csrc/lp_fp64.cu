@@ -159,7 +159,8 @@ double event_s64(cudaEvent_t a, cudaEvent_t b) {
 int validate64(const void* a, int n, int lda, int bs, const char* who) {
     if (a == nullptr) return fail(LP_E_INVALID, std::string(who) + ": null matrix pointer");
     if (n <= 0 || lda < n) return fail(LP_E_INVALID, std::string(who) + ": need n > 0 and lda >= n");
-    if (bs != 64 && bs != 128) return fail(LP_E_INVALID, std::string(who) + ": FP64 block size must be 64 or 128");
+    if (bs != 64 && bs != 128 && bs != 256)
+        return fail(LP_E_INVALID, std::string(who) + ": FP64 block size must be 64, 128 or 256");
     if (n % bs != 0) return fail(LP_E_INVALID, std::string(who) + ": n must be a multiple of the block size");
     if (lda % 2 != 0 || !aligned16(a))
         return fail(LP_E_INVALID, std::string(who) + ": matrix must be 16-byte aligned with an even lda");
@@ -168,21 +169,76 @@ int validate64(const void* a, int n, int lda, int bs, const char* who) {
 
 }  // namespace
 
+// Blocks wider than 128 (256): the same blocked algorithm inside the block
+// with 128-wide inner blocks, as the FP32 path does for its 512 blocks — the
+// lu of the diagonal block recursively, top and left as 128-row / -column
+// exact chunks plus FP64 GEMM updates of the rest.  `dt` holds one transposed
+// 128-wide sub-block (128 x 128) of the diagonal block.
+static int lu_stage64(double* d, int lda, int bs, double* lti, cudaStream_t st) {
+    if (bs <= 128) return launch_lu_small_f64(d, lda, bs, st);
+    const int ib = 128;
+    for (int kk = 0; kk < bs / ib; kk++) {
+        double* dd = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        LP_CHECK(launch_lu_small_f64(dd, lda, ib, st));
+        const int r = bs - (kk + 1) * ib;
+        if (r <= 0) break;
+        LP_CHECK(launch_top_chunk_f64(dd, lda, dd + ib, lda, ib, r, st));
+        LP_CHECK(launch_left_chunk_f64(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, st));
+        LP_CHECK(launch_dgemm_update(dd + (size_t)ib * lda + ib, lda, lti, r, dd + ib, lda, r, r, ib, st));
+    }
+    return LP_OK;
+}
+
+static int top_blocked64(const double* d, int lda, double* t, int ldt, int bs, int ncols, double* dt,
+                         cudaStream_t st) {
+    if (bs <= 128) return launch_top_chunk_f64(d, lda, t, ldt, bs, ncols, st);
+    const int ib = 128;
+    for (int kk = 0; kk < bs / ib; kk++) {
+        const double* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        double* tk = t + (size_t)kk * ib * ldt;
+        LP_CHECK(launch_top_chunk_f64(dkk, lda, tk, ldt, ib, ncols, st));
+        const int m2 = bs - (kk + 1) * ib;
+        if (m2 <= 0) break;
+        // T[below] += D[below][chunk] * T[chunk]: D's sub-block transposed into the k-major operand
+        LP_CHECK(launch_transpose_f64(dkk + (size_t)ib * lda, lda, dt, m2, m2, ib, st));
+        LP_CHECK(launch_dgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, ncols, ib, st));
+    }
+    return LP_OK;
+}
+
+static int left_blocked64(const double* d, int lda, double* l, int ldl, int bs, int nrows, double* lt, int ldlt,
+                          cudaStream_t st) {
+    if (bs <= 128) return launch_left_chunk_f64(d, lda, l, ldl, bs, nrows, lt, ldlt, st);
+    const int ib = 128;
+    for (int kk = 0; kk < bs / ib; kk++) {
+        const double* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+        double* lk = l + (size_t)kk * ib;
+        double* ltk = lt + (size_t)kk * ib * ldlt;
+        LP_CHECK(launch_left_chunk_f64(dkk, lda, lk, ldl, ib, nrows, ltk, ldlt, st));
+        const int m2 = bs - (kk + 1) * ib;
+        if (m2 <= 0) break;
+        // L[:, after] += L[:, chunk] * D[chunk][after]
+        LP_CHECK(launch_dgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, nrows, m2, ib, st));
+    }
+    return LP_OK;
+}
+
 int gefa_f64(lp_ctx* c, double* a, int n, int lda, int bs, cudaStream_t st) {
-    LP_CHECK(c->f64lt.ensure(sizeof(double) * (size_t)bs * n));
+    LP_CHECK(c->f64lt.ensure(sizeof(double) * ((size_t)bs * n + (bs > 128 ? 2 * (size_t)128 * bs : 0))));
     double* lt = static_cast<double*>(c->f64lt.ptr);
+    double* scratch = lt + (size_t)bs * n;  // bs > 128: inner Lt of the lu stage, then transposed D sub-blocks
     for (int k0 = 0; k0 < n; k0 += bs) {
         double* d = a + (size_t)k0 * lda + k0;
         const int rest = n - k0 - bs;
         int e = prof_begin(c, st);
-        LP_CHECK(launch_lu_small_f64(d, lda, bs, st));
+        LP_CHECK(lu_stage64(d, lda, bs, scratch, st));
         LP_CHECK(prof_end(c, st, LP_STAGE_LU, e, 2.0 * bs * bs * bs / 3.0, 16.0 * bs * bs));
         if (rest <= 0) break;
         e = prof_begin(c, st);
-        LP_CHECK(launch_top_chunk_f64(d, lda, d + bs, lda, bs, rest, st));
+        LP_CHECK(top_blocked64(d, lda, d + bs, lda, bs, rest, scratch, st));
         LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, (double)bs * bs * rest, 16.0 * bs * rest));
         e = prof_begin(c, st);
-        LP_CHECK(launch_left_chunk_f64(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
+        LP_CHECK(left_blocked64(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, st));
         LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, (double)bs * bs * rest, 24.0 * bs * rest));
         e = prof_begin(c, st);
         LP_CHECK(launch_dgemm_update(d + (size_t)bs * lda + bs, lda, lt, rest, d + bs, lda, rest, rest, bs, st));
@@ -256,8 +312,8 @@ int lp_calculate_f64(lp_ctx* c, int n, int lda, int bs, int repetitions, double*
     if (c == nullptr || A == nullptr || b == nullptr || gefa_times == nullptr || gesl_times == nullptr)
         return fail(LP_E_INVALID, "lp_calculate_f64: null argument");
     if (repetitions <= 0) return fail(LP_E_INVALID, "lp_calculate_f64: repetitions must be positive");
-    if (n <= 0 || lda < n || lda % 2 != 0 || (bs != 64 && bs != 128) || n % bs != 0)
-        return fail(LP_E_INVALID, "lp_calculate_f64: n a multiple of bs (64 or 128), lda >= n and even");
+    if (n <= 0 || lda < n || lda % 2 != 0 || (bs != 64 && bs != 128 && bs != 256) || n % bs != 0)
+        return fail(LP_E_INVALID, "lp_calculate_f64: n a multiple of bs (64, 128 or 256), lda >= n and even");
     LP_CUDA(cudaSetDevice(c->device));
     const size_t abytes = sizeof(double) * (size_t)n * lda;
     LP_CHECK(c->f64a.ensure(abytes));

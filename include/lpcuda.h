@@ -216,7 +216,7 @@ int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, i
 /* ---- FP64 (the reference's _DP build; device pointers) --------------------
  * The same blocked LU without pivoting and the same encoding in double
  * (DATA_TYPE / HOST_DATA_TYPE double, LINPACK/src/host/parameters.h.in):
- * gefa_ref_nopvt / gesl_ref_nopvt of the double build.  bs 64 or 128, n a
+ * gefa_ref_nopvt / gesl_ref_nopvt of the double build.  bs 64, 128 or 256, n a
  * multiple of bs, lda even, dA 16-byte aligned. */
 int lp_gefa_f64_dev(lp_ctx* ctx, double* dA, int n, int lda, int bs);
 /* Forward + back substitution, nrhs right-hand sides as rows of dB. */

@@ -64,7 +64,7 @@ def test_two_blocks_stages_bitexact(ctx, dev, bs):
     assert tail.max() < 64 * n * DBL_EPS
 
 
-@pytest.mark.parametrize("n,bs", [(256, 64), (1024, 128), (2048, 128)])
+@pytest.mark.parametrize("n,bs", [(256, 64), (1024, 128), (2048, 128), (1024, 256), (2048, 256)])
 def test_factor_and_solve(ctx, dev, n, bs):
     A, b = dominant(n, n)
     got = gpu_gefa(ctx, dev, A, bs)
