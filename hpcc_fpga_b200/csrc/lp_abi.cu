@@ -623,15 +623,25 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
     cudaPointerAttributes pa{};
     const bool pinned = cudaPointerGetAttributes(&pa, A) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();  // an unregistered pointer may leave an error behind
-    std::vector<cudaEvent_t> evs;
+    // the band events, destroyed on every way out (after the copy stream drained)
+    struct Events {
+        std::vector<cudaEvent_t> v;
+        cudaStream_t copy = nullptr;
+        ~Events() {
+            if (copy != nullptr) cudaStreamSynchronize(copy);
+            for (auto e : v)
+                if (e != nullptr) cudaEventDestroy(e);
+        }
+    } evs;
     FactorSink sink;
     if (pinned) {
         if (c->copy == nullptr) LP_CUDA(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
-        evs.resize(n / bs, nullptr);
-        for (auto& e : evs) LP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        evs.copy = c->copy;
+        evs.v.resize(n / bs, nullptr);
+        for (auto& e : evs.v) LP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         sink.host = A;
         sink.copy = c->copy;
-        sink.events = &evs;
+        sink.events = &evs.v;
     }
     int status = LP_OK;
     for (int rep = 0; rep < repetitions && status == LP_OK; rep++) {
@@ -654,11 +664,7 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
         LP_CUDA(cudaMemcpyAsync(b, dB, sizeof(float) * n, cudaMemcpyDeviceToHost, st));
         LP_CUDA(cudaStreamSynchronize(st));
     }
-    if (pinned) {
-        cudaStreamSynchronize(c->copy);
-        for (auto e : evs)
-            if (e != nullptr) cudaEventDestroy(e);
-    }
+    if (pinned && status == LP_OK) LP_CUDA(cudaStreamSynchronize(c->copy));
     return status;
 }
 

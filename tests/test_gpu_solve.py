@@ -35,14 +35,18 @@ def test_calculate_reference_inputs(ctx, bs, blocks):
     assert np.abs(b_dev - 1.0).max() <= 4 * max(np.abs(x_ref - 1.0).max(), n * FLT_EPS)
 
 
-@pytest.mark.parametrize("n,bs,reps", [(1024, 128, 1), (2048, 512, 2)])
-def test_calculate_pinned_overlapped_copy(ctx, lp, n, bs, reps):
+@pytest.mark.parametrize("n,bs,reps,pad", [(1024, 128, 1, 0), (2048, 512, 2, 0), (1024, 256, 1, 8)])
+def test_calculate_pinned_overlapped_copy(ctx, lp, n, bs, reps, pad):
     """Page-locked A: the factors return band by band while later block steps
-    run; the result equals the pageable path's exactly."""
-    A, b, _, _ = oracle.gen_reference(n)
+    run; the result equals the pageable path's exactly (also with lda > n,
+    where the padding columns stay as they were)."""
+    A0, b, _, _ = oracle.gen_reference(n)
+    A = np.full((n, n + pad), 7.0, np.float32)
+    A[:, :n] = A0
     A1, b1 = A.copy(), b.copy()
     ctx.calculate(A1, b1, bs, repetitions=reps)
-    pa, pb = lp.Pinned((n, n)), lp.Pinned((n,))
+    assert np.all(A1[:, n:] == 7.0)
+    pa, pb = lp.Pinned((n, n + pad)), lp.Pinned((n,))
     try:
         pa.array[:] = A
         pb.array[:] = b
