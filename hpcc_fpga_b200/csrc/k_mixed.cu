@@ -1,6 +1,7 @@
-// Mixed-precision factorization: the block schedule of gefa_f32 (lu, top,
-// left in FP32, one step of look-ahead) with the trailing update on the
-// tensor cores (k_umma.cu).  After each panel its left block column L and top
+// Mixed-precision factorization: the block schedule of gefa_f32 (one step of
+// look-ahead) with the trailing update on the tensor cores (k_umma.cu), and
+// the panel's top and left stages as tensor-core products with the inverted
+// triangles of the FP32 diagonal block (panel_tc).  After each panel its left block column L and top
 // block row T are rounded to the tensor-core operand type:
 //   BF16:  Lq[m][k] = bf16(L[m][k]),  Tq[n][k] = bf16(T[k][n]);
 //   E4M3:  one absmax scale per 512-row block of L and per 512-column block
@@ -115,26 +116,37 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16&
     c = __float2bfloat16_rn(r1 - __bfloat162float(b));
 }
 
-// Segment s of the K = 6 k operand row pairs L-term kLseg[s] with T-term kTseg[s].
-__constant__ int kLseg[6] = {2, 1, 0, 1, 0, 0};
-__constant__ int kTseg[6] = {0, 1, 2, 0, 1, 0};
+// Segment s of the K = nseg k operand pairs L-term lterm(s) with T-term
+// tterm(s) (term 0 = x1, the largest).  nseg 6: x3 t1 + x2 t2 + x1 t3 +
+// x2 t1 + x1 t2 + x1 t1 (FP32 accuracy); nseg 3: x2 t1 + x1 t2 + x1 t1
+// (about 2^-16 relative, the three-term split's first two terms).
+template <int NSEG>
+__host__ __device__ constexpr int lterm(int s) {
+    return NSEG == 6 ? (s == 0 ? 2 : (s == 1 || s == 3) ? 1 : 0) : (s == 0 ? 1 : 0);
+}
+template <int NSEG>
+__host__ __device__ constexpr int tterm(int s) {
+    return NSEG == 6 ? (s == 2 ? 2 : (s == 1 || s == 4) ? 1 : 0) : (s == 1 ? 1 : 0);
+}
 
-// out[r][s*k + c] = term kLseg[s] of L[r][c]: rows x (6 k) BF16.
+// out[r][s*k + c] = term lterm(s) of L[r][c]: rows x (NSEG k) BF16.
+template <int NSEG>
 __global__ void k_split_rows(const float* __restrict__ L, int ldl, __nv_bfloat16* __restrict__ out, int rows, int k) {
     const size_t total = (size_t)rows * k;
-    const size_t kq = 6 * (size_t)k;
+    const size_t kq = NSEG * (size_t)k;
     for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
         const int r = (int)(e / k), c = (int)(e - (size_t)r * k);
         __nv_bfloat16 t[3];
         split3(L[(size_t)r * ldl + c], t[0], t[1], t[2]);
         __nv_bfloat16* o = out + (size_t)r * kq + c;
 #pragma unroll
-        for (int s = 0; s < 6; s++) o[(size_t)s * k] = t[kLseg[s]];
+        for (int s = 0; s < NSEG; s++) o[(size_t)s * k] = t[lterm<NSEG>(s)];
     }
 }
 
-// out[c][s*k + r] = term kTseg[s] of T[r][c]: cols x (6 k) BF16, through a
+// out[c][s*k + r] = term tterm(s) of T[r][c]: cols x (NSEG k) BF16, through a
 // 32 x 32 shared-memory transpose.
+template <int NSEG>
 __global__ void __launch_bounds__(256) k_split_trans(const float* __restrict__ T, int ldt,
                                                      __nv_bfloat16* __restrict__ out, int k, int cols) {
     __shared__ float tile[32][33];
@@ -146,7 +158,7 @@ __global__ void __launch_bounds__(256) k_split_trans(const float* __restrict__ T
         tile[ty + j][tx] = (r < k && c < cols) ? T[(size_t)r * ldt + c] : 0.0f;
     }
     __syncthreads();
-    const size_t kq = 6 * (size_t)k;
+    const size_t kq = NSEG * (size_t)k;
 #pragma unroll
     for (int j = 0; j < 32; j += 8) {
         const int c = c0 + ty + j, r = r0 + tx;
@@ -155,22 +167,47 @@ __global__ void __launch_bounds__(256) k_split_trans(const float* __restrict__ T
             split3(tile[tx][ty + j], t[0], t[1], t[2]);
             __nv_bfloat16* o = out + (size_t)c * kq + r;
 #pragma unroll
-            for (int s = 0; s < 6; s++) o[(size_t)s * k] = t[kTseg[s]];
+            for (int s = 0; s < NSEG; s++) o[(size_t)s * k] = t[tterm<NSEG>(s)];
         }
+    }
+}
+
+// x[i][i] += v for i < n (an n x n block, leading dimension n).
+__global__ void k_add_diag(float* __restrict__ x, int n, float v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[(size_t)i * n + i] += v;
+}
+
+// x = identity (two n x n blocks, leading dimension n).
+__global__ void k_eye2(float* __restrict__ x, float* __restrict__ y, int n) {
+    const size_t total = (size_t)n * n;
+    for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+        const float v = (e / n == e % n) ? 1.0f : 0.0f;
+        x[e] = v;
+        y[e] = v;
     }
 }
 
 }  // namespace
 
-// The BF16x6 operands of a block step: aq: rows_l x 6k, bq: cols_t x 6k.
+// The split-BF16 operands of a block step (nseg 6 or 3 K-segments):
+// aq: rows_l x nseg k, bq: cols_t x nseg k.
 int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
-                uint8_t* bq, cudaStream_t st) {
+                uint8_t* bq, cudaStream_t st, int nseg) {
     if (rows_l <= 0 || cols_t <= 0) return LP_OK;
+    if (nseg != 6 && nseg != 3) return fail(LP_E_INVALID, "split_panel: 3 or 6 segments");
     const size_t total = (size_t)rows_l * k;
     const int grid = (int)((total + 255) / 256 < 4736 ? (total + 255) / 256 : 4736);
-    k_split_rows<<<grid, 256, 0, st>>>(L, ldl, reinterpret_cast<__nv_bfloat16*>(aq), rows_l, k);
     const dim3 tgrid((cols_t + 31) / 32, (k + 31) / 32);
-    k_split_trans<<<tgrid, 256, 0, st>>>(T, ldt, reinterpret_cast<__nv_bfloat16*>(bq), k, cols_t);
+    auto* a = reinterpret_cast<__nv_bfloat16*>(aq);
+    auto* b = reinterpret_cast<__nv_bfloat16*>(bq);
+    if (nseg == 6) {
+        k_split_rows<6><<<grid, 256, 0, st>>>(L, ldl, a, rows_l, k);
+        k_split_trans<6><<<tgrid, 256, 0, st>>>(T, ldt, b, k, cols_t);
+    } else {
+        k_split_rows<3><<<grid, 256, 0, st>>>(L, ldl, a, rows_l, k);
+        k_split_trans<3><<<tgrid, 256, 0, st>>>(T, ldt, b, k, cols_t);
+    }
     count_launch(2);
     LP_CUDA(cudaGetLastError());
     return LP_OK;
@@ -221,6 +258,66 @@ static int mixed_update(lp_ctx* c, float* c11, int lda, const uint8_t* aq, const
                               static_cast<int*>(c->err.ptr), st);
 }
 
+// Panel of block step K for the tensor-core schedules.  lu of the diagonal
+// block D as in the FP32 schedule.  top and left are triangular solves with
+// D's two triangles (storage indices, k_trsm.cu):
+//   top:  each column t of the block row satisfies t_k = D_kk (t0_k + sum_{i<k} D_ki t_i),
+//         i.e. t = W^-1 t0 with W = diag(D)^-1 - strict-lower(D);
+//   left: each row l of the block column satisfies l_i = l0_i + sum_{k<i} l_k D_ki,
+//         i.e. l = l0 V with V = (I - strict-upper(D))^-1.
+// W^-1 and V are the two recurrences applied to a bs x bs identity (the exact
+// kernels, a small problem); then T = W^-1 T0 (into the zeroed block row) and
+// L += L (V - I) run as split-BF16 tensor-core products (nseg K-segments), so
+// the n bs^2 flops of the recurrences per step leave the FMA pipe.  V is unit
+// triangular, so L keeps its exact identity part; W^-1 is not (its diagonal
+// is D_kk = -1/u_kk), and T0 + (W^-1 - I) T0 would cancel nearly all of T0.
+static int panel_tc(lp_ctx* c, float* dA, int n, int lda, int bs, int K, int nseg, cudaStream_t s) {
+    float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+    const double b = bs;
+    int e = prof_begin(c, s);
+    LP_CHECK(lu_stage(c, d, lda, bs, s));
+    LP_CHECK(prof_end(c, s, LP_STAGE_LU, e, 2.0 * b * b * b / 3.0, 8.0 * b * b));
+    const int rest = n - (K + 1) * bs;
+    if (rest <= 0) return LP_OK;
+    const double r = rest;
+    const size_t bb = (size_t)bs * bs, kq = (size_t)nseg * bs;
+    float* winv = static_cast<float*>(c->tri.ptr);
+    float* vinv = winv + bb;
+    float* vlt = vinv + bb;
+    __nv_bfloat16* tq = static_cast<__nv_bfloat16*>(c->tq.ptr);
+    uint8_t* a_top = reinterpret_cast<uint8_t*>(tq);                    // bs x kq: W^-1
+    uint8_t* b_left = reinterpret_cast<uint8_t*>(tq + bb * nseg);       // bs x kq: (V - I)^T
+    uint8_t* b_top = reinterpret_cast<uint8_t*>(tq + 2 * bb * nseg);    // rest x kq: T^T
+    uint8_t* a_left = reinterpret_cast<uint8_t*>(tq + 2 * bb * nseg + (size_t)n * kq);  // rest x kq: L
+    int* err = static_cast<int*>(c->err.ptr);
+
+    e = prof_begin(c, s);
+    k_eye2<<<(int)((bb + 255) / 256 < 1184 ? (bb + 255) / 256 : 1184), 256, 0, s>>>(winv, vinv, bs);
+    count_launch();
+    LP_CUDA(cudaGetLastError());
+    LP_CUDA(cudaEventRecord(c->ev_side, s));
+    LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
+    LP_CHECK(left_blocked(d, lda, vinv, bs, bs, bs, vlt, bs, c->aux2));
+    LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
+    LP_CHECK(top_blocked(c, d, lda, winv, bs, bs, bs, s));
+    LP_CUDA(cudaStreamWaitEvent(s, c->ev_side_done, 0));
+    k_add_diag<<<(bs + 127) / 128, 128, 0, s>>>(vinv, bs, -1.0f);
+    count_launch();
+    LP_CUDA(cudaGetLastError());
+    float* t = d + bs;
+    float* l = d + (size_t)bs * lda;
+    LP_CHECK(split_panel(winv, bs, t, lda, bs, rest, bs, a_top, b_top, s, nseg));
+    LP_CUDA(cudaMemset2DAsync(t, sizeof(float) * (size_t)lda, 0, sizeof(float) * (size_t)rest, bs, s));
+    LP_CHECK(launch_umma_update(t, lda, a_top, bs, b_top, rest, 0, 0, bs, rest, (int)kq, false, nullptr, nullptr,
+                                err, s));
+    LP_CHECK(prof_end(c, s, LP_STAGE_TOP, e, b * b * r, 8.0 * b * r));
+    e = prof_begin(c, s);
+    LP_CHECK(split_panel(l, lda, vinv, bs, rest, bs, bs, a_left, b_left, s, nseg));
+    LP_CHECK(launch_umma_update(l, lda, a_left, rest, b_left, bs, 0, 0, rest, bs, (int)kq, false, nullptr, nullptr,
+                                err, s));
+    return prof_end(c, s, LP_STAGE_LEFT, e, b * b * r, 8.0 * b * r);
+}
+
 int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st) {
     const bool fp8 = precision == LP_FP8_IR;
     const bool x6 = precision == LP_F32_BF16X6;
@@ -228,9 +325,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     const size_t esz = fp8 ? 1 : 2;
     const int kq = x6 ? 6 * bs : bs;  // K of the tensor-core update
     const size_t pan = (size_t)kq * n;      // one tensor-core operand
-    const size_t pan_f = (size_t)bs * n;    // one FP32 panel
     const int nblk = (n + 511) / 512;
-    LP_CHECK(c->lt.ensure(2 * sizeof(float) * pan_f));
     if (bs > 128) {
         LP_CHECK(c->lti.ensure(2 * sizeof(float) * (size_t)128 * bs));
         LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
@@ -238,8 +333,12 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     LP_CHECK(c->q.ensure(4 * esz * pan));
     LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)nblk));
     LP_CHECK(c->err.ensure(sizeof(int)));
+    // the top / left products: FP32 accuracy for the emulated-FP32 form, three
+    // segments where the panel is rounded to BF16 / E4M3 afterwards anyway
+    const int nseg = x6 ? 6 : 3;
+    LP_CHECK(c->tri.ensure(3 * sizeof(float) * (size_t)bs * bs));
+    LP_CHECK(c->tq.ensure(2 * sizeof(__nv_bfloat16) * (size_t)nseg * bs * ((size_t)bs + n)));
     LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
-    float* ltbuf[2] = {static_cast<float*>(c->lt.ptr), static_cast<float*>(c->lt.ptr) + pan_f};
     uint8_t* q = static_cast<uint8_t*>(c->q.ptr);
     uint8_t* aqb[2] = {q, q + 2 * esz * pan};
     uint8_t* bqb[2] = {q + esz * pan, q + 3 * esz * pan};
@@ -248,7 +347,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     const double b = bs;
 
     auto panel_q = [&](int K, cudaStream_t s) -> int {
-        LP_CHECK(panel_f32(c, dA, n, lda, bs, K, ltbuf[K & 1], s));
+        LP_CHECK(panel_tc(c, dA, n, lda, bs, K, nseg, s));
         const int rest = n - (K + 1) * bs;
         if (rest <= 0) return LP_OK;
         float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;

@@ -19,7 +19,8 @@
 //               32 x 32 block through shared memory and add it into C with
 //               coalesced loads/stores (the C block is prefetched before the
 //               accumulator is ready).  C is read and written once.
-// The diagonal block and the triangular stages stay FP32 (k_lu.cu, k_trsm.cu).
+// The same kernel runs the mixed schedules' top and left stages as products
+// with the inverted triangles of the diagonal block (k_mixed.cu).
 //
 // Every mbarrier wait is bounded.  On expiry the thread records an error
 // code in *err, raises the CTA's abort flag, stops issuing work, lets its own

@@ -130,7 +130,7 @@ static double inner_bytes(double m, double n, double k) { return 4.0 * (2.0 * m 
 // Larger blocks are factored as the same blocked algorithm with 128-wide
 // inner blocks (lu, top, left, inner on the bs x bs sub-matrix), which keeps
 // every piece on the kernels above and spreads the inner work over the GPU.
-static int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
+int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
     if (bs <= 128) return launch_lu_small(d, lda, bs, st);
     const int ib = 128;
     float* lti = static_cast<float*>(c->lti.ptr);
@@ -157,7 +157,7 @@ static int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
 // (full width, every column strip in parallel), then the chunk's
 // contribution to the rows below as one GEMM, T[below] += D[below][chunk] *
 // T[chunk] (D's sub-block transposed into the k-major operand first).
-static int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols,
+int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols,
                        cudaStream_t st) {
     if (bs <= 128) return launch_trsm_top(d, lda, t, ldt, bs, ncols, st);
     const int ib = 128;
@@ -178,7 +178,7 @@ static int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, in
 // d, and Lt = L^T.  Larger blocks walk 128-column chunks: exact recurrence on
 // the chunk's columns (which also writes the chunk's rows of Lt), then
 // L[:, after] += L[:, chunk] * D[chunk][after] as one GEMM.
-static int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
+int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
                         cudaStream_t st) {
     if (bs <= 128) return launch_trsm_left(d, lda, l, ldl, bs, nrows, lt, ldlt, st);
     const int ib = 128;

@@ -38,9 +38,14 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
 int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st);
 int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
                    uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st);
-// BF16x6 operands (exact three-term split, six K-segments) of a block step.
+// Split-BF16 operands (exact three-term split; 6 or 3 K-segments) of a block step.
 int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
-                uint8_t* bq, cudaStream_t st);
+                uint8_t* bq, cudaStream_t st, int nseg = 6);
+// The stages of panel_f32 (lp_abi.cu): lu of a diagonal block, and the top /
+// left recurrences over a block row / column (Lt written into lt).
+int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st);
+int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st);
+int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, cudaStream_t st);
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
                        int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
                        cudaStream_t st);
@@ -108,6 +113,8 @@ struct lp_ctx {
     lp::Workspace q;     // tensor-core operands: 2 x (Lq, Tq), BF16 or E4M3, n x bs each
     lp::Workspace qs;    // E4M3 block scales (absmax, scale, 1/scale for L and T), 2 buffers
     lp::Workspace err;   // device error word of the tensor-core update (bounded waits)
+    lp::Workspace tri;   // mixed panel: inverses of the diagonal block's triangles (2 x bs x bs) + Lt scratch
+    lp::Workspace tq;    // mixed panel: split-BF16 operands of the top and left products
     lp::Workspace gw;    // substitution work vectors
     lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
@@ -137,7 +144,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
                                 &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
