@@ -195,8 +195,10 @@ int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, 
 }
 
 // Panel work of block step K: lu on the diagonal block, then the top block
-// row and the left block column (Lt written into `lt`).
-int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st) {
+// row and the left block column (Lt written into `lt`, leading dimension the
+// number of rows below).  The left stage covers the rows below the diagonal
+// block up to row_end (default: all n).
+int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st, int row_end) {
     float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
     const double b = bs;
     int e = prof_begin(c, st);
@@ -204,19 +206,23 @@ int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cu
     LP_CHECK(prof_end(c, st, LP_STAGE_LU, e, lu_flops(b), 8.0 * b * b));
     const int rest = n - (K + 1) * bs;
     if (rest <= 0) return LP_OK;
-    const double r = rest;
+    const int below = (row_end < 0 ? n : row_end) - (K + 1) * bs;
     // top on st and left on aux2 run concurrently: both read only the factored
     // diagonal block and write disjoint blocks (top uses st's dsub slot, left Lt)
-    LP_CUDA(cudaEventRecord(c->ev_side, st));
-    LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
-    e = prof_begin(c, c->aux2);
-    LP_CHECK(left_blocked(d, lda, d + (size_t)bs * lda, lda, bs, rest, lt, rest, c->aux2));
-    LP_CHECK(prof_end(c, c->aux2, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
-    LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
+    if (below > 0) {
+        const double r = below;
+        LP_CUDA(cudaEventRecord(c->ev_side, st));
+        LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
+        e = prof_begin(c, c->aux2);
+        LP_CHECK(left_blocked(d, lda, d + (size_t)bs * lda, lda, bs, below, lt, below, c->aux2));
+        LP_CHECK(prof_end(c, c->aux2, LP_STAGE_LEFT, e, trsm_flops(b, r), 12.0 * b * r));
+        LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
+    }
+    const double r = rest;
     e = prof_begin(c, st);
     LP_CHECK(top_blocked(c, d, lda, d + bs, lda, bs, rest, st));
     LP_CHECK(prof_end(c, st, LP_STAGE_TOP, e, trsm_flops(b, r), 8.0 * b * r));
-    LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
+    if (below > 0) LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
     return LP_OK;
 }
 
@@ -229,24 +235,7 @@ int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cu
 // Lt is double-buffered so panel K+1 never overwrites the operand U_b reads.
 // top and left give the reference recurrences' values up to rounding
 // (blocked); the exact recurrences are lp_top_update_dev/lp_left_update_dev.
-// The final bands of block step K (its block row right of and including the
-// diagonal block, its block column below it) to the sink's host mirror.
-static int sink_bands(const FactorSink* s, const float* dA, int n, int lda, int bs, int K, cudaStream_t done_on) {
-    if (s == nullptr) return LP_OK;
-    cudaEvent_t ev = (*s->events)[K];
-    LP_CUDA(cudaEventRecord(ev, done_on));
-    LP_CUDA(cudaStreamWaitEvent(s->copy, ev, 0));
-    const size_t k0 = (size_t)K * bs, pitch = sizeof(float) * (size_t)lda;
-    LP_CUDA(cudaMemcpy2DAsync(s->host + k0 * lda + k0, pitch, dA + k0 * lda + k0, pitch, sizeof(float) * (n - k0), bs,
-                              cudaMemcpyDeviceToHost, s->copy));
-    const int below = n - (int)k0 - bs;
-    if (below > 0)
-        LP_CUDA(cudaMemcpy2DAsync(s->host + (k0 + bs) * lda + k0, pitch, dA + (k0 + bs) * lda + k0, pitch,
-                                  sizeof(float) * bs, below, cudaMemcpyDeviceToHost, s->copy));
-    return LP_OK;
-}
-
-int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, const FactorSink* sink) {
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st) {
     const size_t pan = sizeof(float) * (size_t)bs * n;
     LP_CHECK(c->lt.ensure(2 * pan));
     if (bs > 128) {
@@ -257,7 +246,6 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, cons
     const int nb = n / bs;
     const double b = bs;
     LP_CHECK(panel_f32(c, dA, n, lda, bs, 0, ltbuf[0], st));
-    LP_CHECK(sink_bands(sink, dA, n, lda, bs, 0, st));
     for (int K = 0; K + 1 < nb; K++) {
         const int rest = n - (K + 1) * bs;
         const double r = rest;
@@ -274,7 +262,6 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, cons
         LP_CUDA(cudaEventRecord(c->ev_fork, st));
         LP_CUDA(cudaStreamWaitEvent(c->aux, c->ev_fork, 0));
         LP_CHECK(panel_f32(c, dA, n, lda, bs, K + 1, ltbuf[(K + 1) & 1], c->aux));
-        LP_CHECK(sink_bands(sink, dA, n, lda, bs, K + 1, c->aux));
         LP_CUDA(cudaEventRecord(c->ev_join, c->aux));
         if (rest > bs) {
             const double r2 = rest - bs;
@@ -285,6 +272,177 @@ int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, cons
         }
         LP_CUDA(cudaStreamWaitEvent(st, c->ev_join, 0));
     }
+    return LP_OK;
+}
+
+// ---- row-slab schedule: the factorization fed from page-locked host memory ----
+
+// One lane of the row-slab schedule: a main and a high-priority side stream,
+// their fork / join events, and the double-buffered Lt of the lane's slab.
+struct Lane {
+    cudaStream_t st, aux;
+    cudaEvent_t fork, join;
+    float* lt[2];
+};
+
+// Block rows [K0, K1) (rows [r0, r1) = [K0 bs, K1 bs)) of the blocked LU, on
+// one lane.  First the block steps K < K0 of the rows above, applied to these
+// rows only (left with D_K on their block column K, then their update with
+// block row K over the full width; one step of look-ahead as in gefa_f32),
+// each after panel_done[K]; then the block steps K0..K1-1 restricted to rows
+// < r1, recording panel_done[K] (by band(K, stream)) when block row K is
+// final.  Every element receives the operations of gefa_f32 in the same order
+// (the stages are row- or column-independent, the update adds a k-ordered
+// product per element), so the factors equal gefa_f32's.
+template <class Band>
+static int gefa_rows(lp_ctx* c, float* dA, int n, int lda, int bs, int r0, int r1, const Lane& ln,
+                     const cudaEvent_t* panel_done, Band band) {
+    const int rows = r1 - r0, k0 = r0 / bs, k1 = r1 / bs;
+    const double b = bs, m = rows;
+    float* slab = dA + (size_t)r0 * lda;
+    cudaStream_t st = ln.st, aux = ln.aux;
+    if (k0 > 0) {
+        LP_CUDA(cudaStreamWaitEvent(st, panel_done[0], 0));
+        int e = prof_begin(c, st);
+        LP_CHECK(left_blocked(dA, lda, slab, lda, bs, rows, ln.lt[0], rows, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_LEFT, e, trsm_flops(b, m), 12.0 * b * m));
+        for (int K = 0; K < k0; K++) {
+            // block row K and D_K are final here: panel_done[K] was waited for
+            // before left(K), which precedes this point on st
+            const int c1 = (K + 1) * bs, ncols = n - c1;
+            const float* tK = dA + (size_t)K * bs * lda + c1;  // block row K right of D_K
+            const float* l = ln.lt[K & 1];
+            float* cs = slab + c1;
+            if (K + 1 < k0) {
+                // the slab's block column K+1 first, its left stage beside the rest of the update
+                e = prof_begin(c, st);
+                LP_CHECK(launch_sgemm_update(cs, lda, l, rows, tK, lda, rows, bs, bs, st));
+                LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(m, b, b), inner_bytes(m, b, b)));
+                LP_CUDA(cudaEventRecord(ln.fork, st));
+                LP_CUDA(cudaStreamWaitEvent(aux, ln.fork, 0));
+                LP_CUDA(cudaStreamWaitEvent(aux, panel_done[K + 1], 0));
+                e = prof_begin(c, aux);
+                LP_CHECK(left_blocked(dA + (size_t)c1 * lda + c1, lda, cs, lda, bs, rows, ln.lt[(K + 1) & 1], rows,
+                                      aux));
+                LP_CHECK(prof_end(c, aux, LP_STAGE_LEFT, e, trsm_flops(b, m), 12.0 * b * m));
+                LP_CUDA(cudaEventRecord(ln.join, aux));
+                const double nc = ncols - bs;  // > 0: the slab's own columns lie beyond c1 + bs
+                e = prof_begin(c, st);
+                LP_CHECK(launch_sgemm_update(cs + bs, lda, l, rows, tK + bs, lda, rows, ncols - bs, bs, st));
+                LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(m, nc, b), inner_bytes(m, nc, b)));
+                LP_CUDA(cudaStreamWaitEvent(st, ln.join, 0));
+            } else {
+                const double nc = ncols;
+                e = prof_begin(c, st);
+                LP_CHECK(launch_sgemm_update(cs, lda, l, rows, tK, lda, rows, ncols, bs, st));
+                LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(m, nc, b), inner_bytes(m, nc, b)));
+            }
+        }
+    }
+    LP_CHECK(panel_f32(c, dA, n, lda, bs, k0, ln.lt[k0 & 1], st, r1));
+    LP_CHECK(band(k0, st));
+    for (int K = k0; K + 1 < k1; K++) {
+        const int below = r1 - (K + 1) * bs;  // >= bs
+        const int rest = n - (K + 1) * bs;    // >= below
+        const double rb = below, rc = rest;
+        float* d = dA + (size_t)K * bs * lda + (size_t)K * bs;
+        float* top = d + bs;
+        float* c11 = d + (size_t)bs * lda + bs;
+        const float* l = ln.lt[K & 1];
+        int e = prof_begin(c, st);
+        LP_CHECK(launch_sgemm_update(c11, lda, l, below, top, lda, bs, rest, bs, st));
+        if (below > bs)
+            LP_CHECK(launch_sgemm_update(c11 + (size_t)bs * lda, lda, l + bs, below, top, lda, below - bs, bs, bs, st));
+        LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(b, rc, b) + inner_flops(rb - b, b, b),
+                          inner_bytes(b, rc, b) + inner_bytes(rb - b, b, b)));
+        LP_CUDA(cudaEventRecord(ln.fork, st));
+        LP_CUDA(cudaStreamWaitEvent(aux, ln.fork, 0));
+        LP_CHECK(panel_f32(c, dA, n, lda, bs, K + 1, ln.lt[(K + 1) & 1], aux, r1));
+        LP_CHECK(band(K + 1, aux));
+        LP_CUDA(cudaEventRecord(ln.join, aux));
+        if (below > bs) {
+            const double r2 = below - bs, c2 = rest - bs;
+            e = prof_begin(c, st);
+            LP_CHECK(launch_sgemm_update(c11 + (size_t)bs * lda + bs, lda, l + bs, below, top + bs, lda, below - bs,
+                                         rest - bs, bs, st));
+            LP_CHECK(prof_end(c, st, LP_STAGE_INNER, e, inner_flops(r2, c2, b), inner_bytes(r2, c2, b)));
+        }
+        LP_CUDA(cudaStreamWaitEvent(st, ln.join, 0));
+    }
+    return LP_OK;
+}
+
+// Row-slab boundaries of the streamed factorization: heights 1024, 2048, then
+// 4096 rows (multiples of bs, at least bs), so the first slab's copy is short.
+static std::vector<int> slab_cuts(int n, int bs) {
+    std::vector<int> cuts{0};
+    const int cap = std::max(bs, 4096 / bs * bs);
+    int h = std::max(bs, 1024 / bs * bs);
+    while (cuts.back() < n) {
+        cuts.push_back(std::min(n, cuts.back() + h));
+        h = std::min(cap, 2 * h);
+    }
+    return cuts;
+}
+
+// gefa_f32 on a matrix that is still in page-locked host memory hA: every
+// row slab is queued for copying on the copy-in stream at once (after the
+// work already queued on st), and each slab is factored as soon as it is
+// resident, on two alternating lanes (st with c->aux, and the context's
+// second lane), so that slab s+1 catches up on the finished block steps while
+// slab s runs its own, whose last steps are short.  Panels never run on both
+// lanes at once (a slab's own steps start after the other lane's last panel),
+// so the panel's scratch is shared.  With host_out, every block row goes back
+// to host_out (leading dimension lda) on the copy stream as soon as it is
+// final.  ev: at least 2 n / bs + 2 events.
+int gefa_f32_streamed(lp_ctx* c, const float* hA, float* dA, int n, int lda, int bs, cudaStream_t st,
+                      float* host_out, const std::vector<cudaEvent_t>& ev) {
+    const std::vector<int> cuts = slab_cuts(n, bs);
+    const int ns = (int)cuts.size() - 1, nb = n / bs;
+    if ((int)ev.size() < nb + ns + 2) return fail(LP_E_INVALID, "streamed factorization: too few events");
+    int hmax = 0;
+    for (int s = 0; s < ns; s++) hmax = std::max(hmax, cuts[s + 1] - cuts[s]);
+    const size_t ltf = (size_t)bs * hmax;
+    LP_CHECK(c->lt.ensure(4 * sizeof(float) * ltf));
+    if (bs > 128) {
+        LP_CHECK(c->lti.ensure(2 * sizeof(float) * (size_t)128 * bs));
+        LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
+    }
+    if (c->copy_in == nullptr) LP_CUDA(cudaStreamCreateWithFlags(&c->copy_in, cudaStreamNonBlocking));
+    if (host_out != nullptr && c->copy == nullptr) LP_CUDA(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+    float* lt = static_cast<float*>(c->lt.ptr);
+    const Lane lanes[2] = {{st, c->aux, c->ev_fork, c->ev_join, {lt, lt + ltf}},
+                           {c->lane_st, c->lane_aux, c->lane_fork, c->lane_join, {lt + 2 * ltf, lt + 3 * ltf}}};
+    const size_t pitch = sizeof(float) * (size_t)lda;
+    // events: block rows' panels ev[0 .. nb), slab arrivals ev[nb .. nb + ns),
+    // start ev[nb + ns], the second lane's end ev[nb + ns + 1]
+    cudaEvent_t ev_start = ev[nb + ns], ev_lane_end = ev[nb + ns + 1];
+    LP_CUDA(cudaEventRecord(ev_start, st));
+    LP_CUDA(cudaStreamWaitEvent(c->copy_in, ev_start, 0));
+    for (int s = 0; s < ns; s++) {
+        const size_t r0 = (size_t)cuts[s];
+        LP_CUDA(cudaMemcpy2DAsync(dA + r0 * lda, pitch, hA + r0 * lda, pitch, sizeof(float) * n, cuts[s + 1] - cuts[s],
+                                  cudaMemcpyHostToDevice, c->copy_in));
+        LP_CUDA(cudaEventRecord(ev[nb + s], c->copy_in));
+    }
+    auto band = [&](int K, cudaStream_t done_on) -> int {
+        LP_CUDA(cudaEventRecord(ev[K], done_on));
+        if (host_out == nullptr) return LP_OK;
+        LP_CUDA(cudaStreamWaitEvent(c->copy, ev[K], 0));
+        const size_t r = (size_t)K * bs;
+        LP_CUDA(cudaMemcpy2DAsync(host_out + r * lda, pitch, dA + r * lda, pitch, sizeof(float) * n, bs,
+                                  cudaMemcpyDeviceToHost, c->copy));
+        return LP_OK;
+    };
+    // the second lane starts after the work queued on st so far
+    LP_CUDA(cudaStreamWaitEvent(c->lane_st, ev_start, 0));
+    for (int s = 0; s < ns; s++) {
+        const Lane& ln = lanes[s & 1];
+        LP_CUDA(cudaStreamWaitEvent(ln.st, ev[nb + s], 0));
+        LP_CHECK(gefa_rows(c, dA, n, lda, bs, cuts[s], cuts[s + 1], ln, ev.data(), band));
+    }
+    LP_CUDA(cudaEventRecord(ev_lane_end, c->lane_st));
+    LP_CUDA(cudaStreamWaitEvent(st, ev_lane_end, 0));
     return LP_OK;
 }
 
@@ -382,6 +540,10 @@ int lp_ctx_create(int device, lp_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_side, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_side_done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_block, cudaEventDisableTiming | cudaEventBlockingSync);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->lane_st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->lane_aux, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->lane_join, cudaEventDisableTiming);
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         lp_ctx_destroy(c);
@@ -398,6 +560,9 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c->aux != nullptr) cudaStreamSynchronize(c->aux);
     if (c->aux2 != nullptr) cudaStreamSynchronize(c->aux2);
     if (c->copy != nullptr) cudaStreamSynchronize(c->copy);
+    if (c->copy_in != nullptr) cudaStreamSynchronize(c->copy_in);
+    if (c->lane_st != nullptr) cudaStreamSynchronize(c->lane_st);
+    if (c->lane_aux != nullptr) cudaStreamSynchronize(c->lane_aux);
     c->release_all();
     for (int i = 0; i < 8; i++)
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
@@ -407,6 +572,11 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c->ev_side_done != nullptr) cudaEventDestroy(c->ev_side_done);
     if (c->aux2 != nullptr) cudaStreamDestroy(c->aux2);
     if (c->copy != nullptr) cudaStreamDestroy(c->copy);
+    if (c->copy_in != nullptr) cudaStreamDestroy(c->copy_in);
+    if (c->lane_fork != nullptr) cudaEventDestroy(c->lane_fork);
+    if (c->lane_join != nullptr) cudaEventDestroy(c->lane_join);
+    if (c->lane_aux != nullptr) cudaStreamDestroy(c->lane_aux);
+    if (c->lane_st != nullptr) cudaStreamDestroy(c->lane_st);
     if (c->ev_block != nullptr) cudaEventDestroy(c->ev_block);
     if (c->aux != nullptr) cudaStreamDestroy(c->aux);
     if (c->stream != nullptr) cudaStreamDestroy(c->stream);
@@ -617,39 +787,42 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
     float* dA = static_cast<float*>(c->dA.ptr);
     float* dB = static_cast<float*>(c->dB.ptr);
     cudaStream_t st = c->stream;
-    // Page-locked A: the last repetition's factors go back to the host band by
-    // band on a copy stream while the later block steps run (execution_pcie.hpp
-    // copies them after the loop, :695-696).  Pageable A: one copy at the end.
+    // Page-locked A: the factorization reads A in row slabs while it runs
+    // (gefa_f32_streamed), and on the last repetition every block row goes back
+    // to A as soon as it is final (execution_pcie.hpp copies A to the device
+    // before and back after the loop, :695-696).  Pageable A: one copy each way.
     cudaPointerAttributes pa{};
     const bool pinned = cudaPointerGetAttributes(&pa, A) == cudaSuccess && pa.type == cudaMemoryTypeHost;
     cudaGetLastError();  // an unregistered pointer may leave an error behind
-    // the band events, destroyed on every way out (after the copy stream drained)
+    // the slab / band events, destroyed on every way out after the copy streams drained
     struct Events {
         std::vector<cudaEvent_t> v;
-        cudaStream_t copy = nullptr;
+        lp_ctx* c = nullptr;
         ~Events() {
-            if (copy != nullptr) cudaStreamSynchronize(copy);
+            if (c != nullptr && c->copy_in != nullptr) cudaStreamSynchronize(c->copy_in);
+            if (c != nullptr) cudaStreamSynchronize(c->lane_st);
+            if (c != nullptr && c->copy != nullptr) cudaStreamSynchronize(c->copy);
             for (auto e : v)
                 if (e != nullptr) cudaEventDestroy(e);
         }
     } evs;
-    FactorSink sink;
     if (pinned) {
-        if (c->copy == nullptr) LP_CUDA(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
-        evs.copy = c->copy;
-        evs.v.resize(n / bs, nullptr);
+        evs.c = c;
+        evs.v.resize(2 * (size_t)(n / bs) + 2, nullptr);
         for (auto& e : evs.v) LP_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        sink.host = A;
-        sink.copy = c->copy;
-        sink.events = &evs.v;
     }
     int status = LP_OK;
     for (int rep = 0; rep < repetitions && status == LP_OK; rep++) {
         const bool last = rep + 1 == repetitions;
-        LP_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, st));
         LP_CUDA(cudaMemcpyAsync(dB, b, sizeof(float) * n, cudaMemcpyHostToDevice, st));
-        LP_CUDA(cudaEventRecord(c->ev[0], st));
-        status = gefa_f32(c, dA, n, lda, bs, st, pinned && last ? &sink : nullptr);
+        if (pinned) {
+            LP_CUDA(cudaEventRecord(c->ev[0], st));
+            status = gefa_f32_streamed(c, A, dA, n, lda, bs, st, last ? A : nullptr, evs.v);
+        } else {
+            LP_CUDA(cudaMemcpyAsync(dA, A, abytes, cudaMemcpyHostToDevice, st));
+            LP_CUDA(cudaEventRecord(c->ev[0], st));
+            status = gefa_f32(c, dA, n, lda, bs, st);
+        }
         if (status != LP_OK) break;
         LP_CUDA(cudaEventRecord(c->ev[1], st));
         status = gesl_f32(c, dA, n, lda, dB, 1, n, st);

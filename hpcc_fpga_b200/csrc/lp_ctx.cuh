@@ -24,18 +24,16 @@ struct Workspace {
 };
 
 int validate_matrix(const void* a, int n, int lda, int bs, const char* who);
-// Optional destination of the factors while they are computed: after each
-// block step's panel its final row and column bands are copied to host (a
-// pinned mirror of dA, leading dimension lda) on the copy stream.
-struct FactorSink {
-    float* host = nullptr;
-    cudaStream_t copy = nullptr;
-    std::vector<cudaEvent_t>* events = nullptr;  // one per block step
-};
-int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st, const FactorSink* sink = nullptr);
+int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st);
+// gefa_f32 on a matrix still in page-locked host memory hA, copied in row slabs
+// while the factorization runs; block rows return to host_out (if not null)
+// as they become final.  ev: 2 n / bs + 2 events.
+int gefa_f32_streamed(lp_ctx* c, const float* hA, float* dA, int n, int lda, int bs, cudaStream_t st,
+                      float* host_out, const std::vector<cudaEvent_t>& ev);
 int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cudaStream_t st);
-// Panel work of block step K (lu, top, left; Lt into lt), on stream st.
-int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st);
+// Panel work of block step K (lu, top, left; Lt into lt), on stream st; the
+// left stage covers the rows below the diagonal block up to row_end (-1: n).
+int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st, int row_end = -1);
 int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
                    uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st);
 // Split-BF16 operands (exact three-term split; 6 or 3 K-segments) of a block step.
@@ -104,6 +102,9 @@ struct lp_ctx {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaStream_t aux2 = nullptr;              // third stream: the left update runs here beside the top update
     cudaStream_t copy = nullptr;              // device-to-host copies of finished factor bands (lp_calculate)
+    cudaStream_t copy_in = nullptr;           // host-to-device copies of the matrix's row slabs (lp_calculate)
+    cudaStream_t lane_st = nullptr, lane_aux = nullptr;  // second lane of the row-slab schedule
+    cudaEvent_t lane_fork = nullptr, lane_join = nullptr;
     cudaEvent_t ev_side = nullptr, ev_side_done = nullptr;
     cudaEvent_t ev_block = nullptr;           // blocking-sync event: waits yield the CPU instead of spinning
     cudaEvent_t ev[8] = {nullptr};

@@ -35,11 +35,15 @@ def test_calculate_reference_inputs(ctx, bs, blocks):
     assert np.abs(b_dev - 1.0).max() <= 4 * max(np.abs(x_ref - 1.0).max(), n * FLT_EPS)
 
 
-@pytest.mark.parametrize("n,bs,reps,pad", [(1024, 128, 1, 0), (2048, 512, 2, 0), (1024, 256, 1, 8)])
+@pytest.mark.parametrize("n,bs,reps,pad", [(1024, 128, 1, 0), (2048, 512, 2, 0), (1024, 256, 1, 8),
+                                           (4096, 128, 1, 0), (3328, 256, 1, 4), (8192, 512, 2, 16)])
 def test_calculate_pinned_overlapped_copy(ctx, lp, n, bs, reps, pad):
-    """Page-locked A: the factors return band by band while later block steps
-    run; the result equals the pageable path's exactly (also with lda > n,
-    where the padding columns stay as they were)."""
+    """Page-locked A: the matrix is copied in row slabs (1024, 2048, then 4096
+    rows) while the factorization runs, each slab catching up on the block
+    steps of the rows above on one of two alternating lanes, and every block
+    row returns as soon as it is final; the result equals the pageable path's
+    (gefa_f32) exactly, also with lda > n (the padding columns stay as they
+    were) and a ragged last slab."""
     A0, b, _, _ = oracle.gen_reference(n)
     A = np.full((n, n + pad), 7.0, np.float32)
     A[:, :n] = A0
