@@ -123,6 +123,19 @@ def cpu_baseline(n: int, reps: int) -> dict:
             "t_min_s": r["t_min"], "host_nproc": os.cpu_count()}
 
 
+def mixed_block(n: int, bs: int) -> int:
+    """Block size of the tensor-core schedules: the largest power of two that
+    leaves at least 32 block steps, at most 2048 and not below the FP32 block.
+    Their update reads and writes FP32 C once per block step, so a wider block
+    cuts that traffic; the panel chain grows with it.  Measured on one B200
+    (BF16+IR): n=65536 block 512 / 1024 / 2048 -> 423 / 536 / 570 TFLOP/s;
+    n=32768 -> 300 / 328 / 313."""
+    b = 1
+    while b * 2 <= min(2048, n // 32):
+        b *= 2
+    return max(bs, b)
+
+
 def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, f32_value, pk) -> dict:
     """BF16 / FP8 trailing updates + FP64 refinement to the HPL threshold on
     the same system: GFLOP/s by the same formula over factor + all solves +
@@ -170,17 +183,30 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, 
     gbs = inner["bytes"] / inner["s"] / 1e9 if inner["s"] > 0 else None
     tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
     value = steps * flops(n) / t / 1e9
+    # The update reads and writes FP32 C once (8 B per element) for 2*bs flop per element:
+    # intensity bs/4 flop/B.  Below the ridge (tensor peak / HBM peak) the launch is
+    # HBM-bound, above it tensor-bound.  No FP8 peak is measured: FP8 counts as twice
+    # the measured BF16 rate (the part's nominal ratio).
+    tpk = pk["bf16_tflops"] * (2.0 if prec == "fp8" else 1.0)
+    ridge = tpk * 1e12 / (pk["hbm_gbs"] * 1e9)
+    tensor_bound = bs / 4.0 > ridge
     return {
         "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32": value / f32_value,
         "ir_iters": max(iters), "hpl_resid": max(resid), "hpl_eps": "DBL_EPSILON/2",
         "max_abs_err_vs_fp64_oracle": float(np.abs(x - 1.0).max()),
-        "roofline": {"bound": "hbm", "kernel": f"k_umma_update<{prec}> (inner stage, tcgen05)",
-                     "achieved": gbs, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                     "frac": gbs / pk["hbm_gbs"] if gbs else None,
-                     "per_unit": "8*m*n bytes (FP32 C read+write) per m x n trailing update; "
-                                 "2*m*n*bs flop, intensity bs/4 flop/B below the BF16 ridge",
-                     "tensor_tflops": tfs, "tensor_peak_tflops": pk["bf16_tflops"],
-                     "peak_source": pk["source"]},
+        "roofline": {"bound": "tensor" if tensor_bound else "hbm",
+                     "kernel": f"k_umma_update<{prec}> (inner stage, tcgen05)",
+                     "achieved": tfs if tensor_bound else gbs,
+                     "peak": tpk if tensor_bound else pk["hbm_gbs"],
+                     "unit": "TFLOP/s" if tensor_bound else "GB/s",
+                     "frac": (tfs / tpk if tensor_bound else gbs / pk["hbm_gbs"]) if gbs else None,
+                     "hbm_frac": gbs / pk["hbm_gbs"] if gbs else None,
+                     "tensor_frac": tfs / tpk if tfs else None,
+                     "per_unit": f"8*m*n bytes (FP32 C read+write) and 2*m*n*{bs} flop per m x n trailing "
+                                 f"update: intensity {bs / 4:.0f} flop/B against the {prec} ridge {ridge:.0f} flop/B",
+                     "tensor_tflops": tfs, "tensor_peak_tflops": tpk,
+                     "peak_source": pk["source"] + ("; FP8 peak = 2 x the measured BF16 rate" if prec == "fp8"
+                                                    else "")},
         "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]},
         "gmres": gmres,
     }
@@ -223,9 +249,10 @@ def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, steps, warm
     tf32eq = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
     value = steps * flops(n) / t / 1e9
     return {
-        "workload": f"the FP32 workload (n={n}, block {bs}, same system and step) with the trailing update "
-                    "emulated on the BF16 tensor cores: exact 3-term BF16 split, 6 products, FP32 accumulation; "
-                    "plain FP32 solve, no refinement",
+        "workload": f"the FP32 workload's system and step (n={n}) in blocks of {bs}, with the trailing update "
+                    "and the panel's top/left products emulated on the BF16 tensor cores: exact 3-term BF16 split, "
+                    "6 products, FP32 accumulation; plain FP32 solve, no refinement",
+        "block": bs,
         "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32_simt": value / f32_value,
         "max_abs_err_x": float(np.abs(x - 1.0).max()),
         "hpl_resid": {"eps_flt_half": r32 * 2.0 ** -29, "eps_dbl_half": r32},
@@ -517,6 +544,9 @@ def main() -> None:
     ap.add_argument("--no-pivot", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-f32emu", action="store_true")
+    ap.add_argument("--mixed-bs", type=int, default=None,
+                    help="block size of the tensor-core schedules (BF16/FP8 + IR, emulated FP32); "
+                         "default: the largest power of two leaving >= 32 block steps, at most 2048")
     ap.add_argument("--serve-rates", default="100,200,300,400,500,600,700,800,900,1000,1250,1500,2000,5000,20000")
     ap.add_argument("--serve-precisions", default="f32,bf16")
     args = ap.parse_args()
@@ -601,15 +631,17 @@ def main() -> None:
     gesl = prof["gesl"]
     pk = peaks()
 
+    mbs = args.mixed_bs or mixed_block(n, bs)
     mixed = {}
-    if not args.no_mixed and bs % 128 == 0:
+    if not args.no_mixed and mbs % 128 == 0:
         for prec in ("bf16", "fp8"):
-            mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, args.steps,
+            mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, mbs, prec, args.steps,
                                     max(1, min(args.warmup, 2)), value / world, pk)
+            mixed[prec]["block"] = mbs
 
     f32emu = None
-    if not args.no_f32emu and bs % 128 == 0:
-        f32emu = run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, args.steps,
+    if not args.no_f32emu and mbs % 128 == 0:
+        f32emu = run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, mbs, args.steps,
                             max(1, min(args.warmup, 2)), value / world, pk)
 
     pivot = None

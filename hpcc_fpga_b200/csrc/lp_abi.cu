@@ -56,11 +56,12 @@ int wait_stream(lp_ctx* c, cudaStream_t st) {
     return LP_OK;
 }
 
-int validate_matrix(const void* a, int n, int lda, int bs, const char* who) {
+int validate_matrix(const void* a, int n, int lda, int bs, const char* who, int max_bs) {
     if (a == nullptr) return fail(LP_E_INVALID, std::string(who) + ": null matrix pointer");
     if (n <= 0) return fail(LP_E_INVALID, std::string(who) + ": n must be positive");
-    if (!is_pow2(bs) || bs < 16 || bs > 512)
-        return fail(LP_E_INVALID, std::string(who) + ": block size must be a power of two in [16, 512]");
+    if (!is_pow2(bs) || bs < 16 || bs > max_bs)
+        return fail(LP_E_INVALID,
+                    std::string(who) + ": block size must be a power of two in [16, " + std::to_string(max_bs) + "]");
     if (n % bs != 0) return fail(LP_E_INVALID, std::string(who) + ": n must be a multiple of the block size");
     if (lda < n || lda % 4 != 0)
         return fail(LP_E_INVALID, std::string(who) + ": lda must be >= n and a multiple of 4");
@@ -710,7 +711,7 @@ int lp_gesl_dev(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs
 
 int lp_gefa_prec_dev(lp_ctx* c, int precision, float* dA, int n, int lda, int bs) {
     if (c == nullptr) return fail(LP_E_INVALID, "lp_gefa_prec_dev: null context");
-    LP_CHECK(validate_matrix(dA, n, lda, bs, "lp_gefa_prec_dev"));
+    LP_CHECK(validate_matrix(dA, n, lda, bs, "lp_gefa_prec_dev", precision == LP_F32 ? 512 : kMixedMaxBlock));
     if (!aligned16(dA)) return fail(LP_E_INVALID, "lp_gefa_prec_dev: matrix must be 16-byte aligned");
     if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR && precision != LP_F32_BF16X6)
         return fail(LP_E_INVALID, "lp_gefa_prec_dev: unknown precision");
@@ -844,7 +845,7 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
 int lp_solve_host(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                   double* x, int max_iters, lp_timing* t) {
     if (c == nullptr || b64 == nullptr || x == nullptr) return fail(LP_E_INVALID, "lp_solve_host: null argument");
-    LP_CHECK(validate_matrix(A, n, lda, bs, "lp_solve_host"));
+    LP_CHECK(validate_matrix(A, n, lda, bs, "lp_solve_host", precision == LP_F32 ? 512 : kMixedMaxBlock));
     if (nrhs <= 0) return fail(LP_E_INVALID, "lp_solve_host: nrhs must be positive");
     if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR && precision != LP_F32_BF16X6)
         return fail(LP_E_INVALID, "lp_solve_host: unknown precision");

@@ -23,7 +23,10 @@ struct Workspace {
     void release();
 };
 
-int validate_matrix(const void* a, int n, int lda, int bs, const char* who);
+// bs: a power of two in [16, max_bs]; 512 is the reference's largest block
+// (the FP32 path), the tensor-core schedules take up to kMixedMaxBlock.
+constexpr int kMixedMaxBlock = 2048;
+int validate_matrix(const void* a, int n, int lda, int bs, const char* who, int max_bs = 512);
 int gefa_f32(lp_ctx* c, float* dA, int n, int lda, int bs, cudaStream_t st);
 // gefa_f32 on a matrix still in page-locked host memory hA, copied in row slabs
 // while the factorization runs; block rows return to host_out (if not null)

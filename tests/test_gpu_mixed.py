@@ -9,6 +9,8 @@ accumulation bound (bs + 2) * eps32 * (|C| + |q(L)| |q(T)|).
 Solve parity: refinement must reach the HPL scaled residual <= 16
 (LINPACK/src/host/gmres.c:182-193) and the FP64-oracle error (the exact
 solution is all ones) must be small."""
+import functools
+
 import numpy as np
 import pytest
 
@@ -76,16 +78,23 @@ def test_gefa_prec_f32_is_gefa(ctx, dev):
     assert np.array_equal(dev.get(d1), dev.get(d2))
 
 
+@functools.lru_cache(maxsize=None)
+def _fp32_factors(n):
+    A, _, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
+    return oracle.gefa_nopvt(A).astype(np.float64)
+
+
 @pytest.mark.parametrize("prec", ["bf16", "fp8"])
-@pytest.mark.parametrize("n,bs", [(1024, 128), (2048, 512)])
+@pytest.mark.parametrize("n,bs", [(1024, 128), (2048, 512), (4096, 1024), (4096, 2048)])
 def test_mixed_factors_close_to_fp32(ctx, dev, prec, n, bs):
     """The rounded-update factors stay close to the FP32 ones (diagonally
-    dominant input: relative error of a few operand roundings)."""
+    dominant input: relative error of a few operand roundings).  Blocks above
+    512 (the FP32 path's largest) are the tensor-core schedules' own."""
     A, _, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
     d = dev.put(A)
     ctx.gefa_prec(prec, d.data_ptr(), n, n, bs)
     got = dev.get(d).astype(np.float64)
-    want = oracle.gefa_nopvt(A).astype(np.float64)
+    want = _fp32_factors(n)
     assert np.all(np.isfinite(got))
     rel = np.abs(got - want).max() / np.abs(want).max()
     assert rel < (2e-2 if prec == "fp8" else 2e-3)
@@ -115,6 +124,32 @@ def test_refine_dev_on_resident_factors(ctx, dev):
     X = dev.get(dX)
     assert t["hpl_resid"] <= 16.0
     assert np.abs(X[0] - 1.0).max() < 1e-9 and np.abs(X[1] - 2.0).max() < 2e-9
+
+
+@pytest.mark.parametrize("prec", ["bf16", "fp8"])
+@pytest.mark.parametrize("bs", [1024, 2048])
+def test_mixed_large_blocks_reach_hpl_threshold(ctx, prec, bs):
+    """Blocks of 1024 and 2048 (half / a quarter of the FP32 C traffic of
+    block 512 per trailing element) refine to the same accuracy."""
+    n = 4096
+    A, b64, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
+    x, t = ctx.solve_host(A, b64, bs, prec, max_iters=50)
+    assert t["hpl_resid"] <= 16.0
+    assert oracle.hpl_resid(A, x, b64) <= 16.0
+    assert np.abs(x - 1.0).max() < 1e-9
+
+
+def test_block_limits_per_path(ctx, dev, lp):
+    """The FP32 path keeps the reference's block range [16, 512]; the
+    tensor-core schedules take up to 2048 and no more."""
+    n = 4096
+    d = dev.put(np.eye(n, dtype=np.float32) * 2)
+    with pytest.raises(lp.LpError) as e:
+        ctx.gefa(d.data_ptr(), n, n, 1024)
+    assert e.value.status == lp.LP_E_INVALID
+    with pytest.raises(lp.LpError) as e:
+        ctx.gefa_prec("bf16", d.data_ptr(), n, n, 4096)
+    assert e.value.status == lp.LP_E_INVALID
 
 
 def test_mixed_rejects_small_block(ctx, lp):
