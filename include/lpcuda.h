@@ -169,8 +169,10 @@ int lp_inner_update_tc_dev(lp_ctx* ctx, int precision, float* dC, int ldc, const
  * n must be a multiple of bs. */
 int lp_gefa_dev(lp_ctx* ctx, float* dA, int n, int lda, int bs);
 /* The same factorization with the trailing updates in the chosen precision
- * (LP_F32: identical to lp_gefa_dev; LP_BF16_IR / LP_FP8_IR: tensor-core
- * trailing updates, bs a multiple of 128; the factors stay FP32). */
+ * (LP_F32: identical to lp_gefa_dev, bs 16..512; LP_BF16_IR / LP_FP8_IR /
+ * LP_F32_BF16X6: tensor-core trailing updates and top/left products, bs a
+ * power of two in 128..2048 — a wider block cuts the FP32 traffic of the
+ * trailing updates; the factors stay FP32). */
 int lp_gefa_prec_dev(lp_ctx* ctx, int precision, float* dA, int n, int lda, int bs);
 /* x = LU \ b followed by FP64 iterative refinement: r = b - M x with the
  * original FP32 matrix dA0 widened to FP64, d = LU \ r, x += d, until the
@@ -268,7 +270,8 @@ int lp_calculate_pvt(lp_ctx* ctx, int n, int lda, int repetitions, float* A, flo
  * the chosen precision; copies are part of the call and are timed in t.
  * For LP_F32, x = the FP32 solve widened to double; for the mixed
  * precisions, x is refined in FP64 against b64 (FP64 right-hand sides,
- * rows of length n) until the HPL scaled residual is <= 16 or max_iters. */
+ * rows of length n) until the HPL scaled residual is <= 16 or max_iters.
+ * bs: as for lp_gefa_prec_dev (16..512 for LP_F32, 128..2048 otherwise). */
 int lp_solve_host(lp_ctx* ctx, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                   double* x, int max_iters, lp_timing* t);
 
