@@ -783,6 +783,7 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
     if (repetitions <= 0) return fail(LP_E_INVALID, "lp_calculate: repetitions must be positive");
     LP_CUDA(cudaSetDevice(c->device));
     const size_t abytes = sizeof(float) * (size_t)n * lda;
+    c->fac_n = 0;  // dA is reused: factors of an earlier lp_factor are gone
     LP_CHECK(c->dA.ensure(abytes));
     LP_CHECK(c->dB.ensure(sizeof(float) * (size_t)n));
     float* dA = static_cast<float*>(c->dA.ptr);
@@ -840,6 +841,24 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
     }
     if (pinned && status == LP_OK) LP_CUDA(cudaStreamSynchronize(c->copy));
     return status;
+}
+
+int lp_factor(lp_ctx* c, int precision, int n, int bs, float* A, int lda, lp_timing* t) {
+    if (c == nullptr) return fail(LP_E_INVALID, "lp_factor: null context");
+    if (precision != LP_F32 && precision != LP_BF16_IR && precision != LP_FP8_IR && precision != LP_F32_BF16X6)
+        return fail(LP_E_INVALID, "lp_factor: unknown precision");
+    LP_CHECK(validate_matrix(A, n, lda, bs, "lp_factor", precision == LP_F32 ? 512 : kMixedMaxBlock));
+    LP_CUDA(cudaSetDevice(c->device));
+    return factor_host_impl(c, precision, n, bs, A, lda, t);
+}
+
+int lp_solve(lp_ctx* c, int n, int nrhs, const float* B, double* X, lp_timing* t) {
+    if (c == nullptr || B == nullptr || X == nullptr) return fail(LP_E_INVALID, "lp_solve: null argument");
+    if (c->fac_n <= 0) return fail(LP_E_INVALID, "lp_solve: no resident factors (call lp_factor first)");
+    if (n != c->fac_n) return fail(LP_E_INVALID, "lp_solve: n differs from the factored matrix");
+    if (nrhs <= 0) return fail(LP_E_INVALID, "lp_solve: nrhs must be positive");
+    LP_CUDA(cudaSetDevice(c->device));
+    return solve_resident_impl(c, nrhs, B, X, t);
 }
 
 int lp_solve_host(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,

@@ -88,6 +88,12 @@ int gmres_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, cons
 int wait_stream(lp_ctx* c, cudaStream_t st);
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                     double* x, int max_iters, lp_timing* t);
+// lp_factor / lp_solve: factors of a host matrix kept resident in the context
+// (dA, with the original in dA0) between the two calls.
+int factor_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, lp_timing* t);
+int solve_resident_impl(lp_ctx* c, int nrhs, const float* B, double* X, lp_timing* t);
+// Refinements lp_solve allows the tensor-core precisions.
+constexpr int kSolveMaxRefinements = 50;
 
 // Stage profiling: prof_begin returns an event index (or -1 when profiling
 // is off); prof_end records the closing event and the stage's work.
@@ -122,6 +128,7 @@ struct lp_ctx {
     lp::Workspace gw;    // substitution work vectors
     lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
+    int fac_n = 0, fac_lda = 0, fac_prec = -1;  // factors resident in dA (lp_factor); fac_n 0: none
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
     lp::Workspace dnorm;                      // refinement norms (device)
     unsigned long long* hnorm = nullptr;      // their pinned host copy

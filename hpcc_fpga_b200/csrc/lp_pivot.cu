@@ -123,6 +123,7 @@ int lp_calculate_pvt(lp_ctx* c, int n, int lda, int repetitions, float* A, float
     if (repetitions <= 0) return fail(LP_E_INVALID, "lp_calculate_pvt: repetitions must be positive");
     LP_CUDA(cudaSetDevice(c->device));
     const size_t abytes = sizeof(float) * (size_t)n * lda;
+    c->fac_n = 0;  // dA is reused: factors of an earlier lp_factor are gone
     LP_CHECK(c->dA.ensure(abytes));
     LP_CHECK(c->dB.ensure(sizeof(float) * (size_t)n));
     LP_CHECK(c->pipvt.ensure(sizeof(int) * (size_t)n));

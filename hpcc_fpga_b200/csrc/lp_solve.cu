@@ -4,7 +4,8 @@
 // until the HPL scaled residual (LINPACK/src/host/gmres.c:182-193,
 // eps = DBL_EPSILON/2) is <= 16 or max_iters refinements were made.  The
 // residual and the update are the only FP64 steps.  lp_solve_host wraps it
-// with the factorization and the host copies.
+// with the factorization and the host copies; lp_factor / lp_solve split the
+// two, keeping the factors resident in between.
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -99,6 +100,7 @@ int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, con
 
 int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                     double* x, int max_iters, lp_timing* t) {
+    c->fac_n = 0;  // dA / dA0 are reused below: factors of an earlier lp_factor are gone
     cudaStream_t st = c->stream;
     const size_t abytes = sizeof(float) * (size_t)n * lda;
     const size_t nv = (size_t)n * nrhs;
@@ -133,6 +135,77 @@ int solve_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, 
         t->h2d_s = ev_s(c->ev[0], c->ev[1]);
         t->gefa_s = ev_s(c->ev[2], c->ev[3]);
         t->gesl_s = ev_s(c->ev[3], c->ev[4]);
+        t->ir_s = ev_s(c->ev[4], c->ev[5]);
+        t->d2h_s = ev_s(c->ev[5], c->ev[6]);
+        t->ir_iters = iters;
+        t->hpl_resid = resid;
+    }
+    return s;
+}
+
+// lp_factor: A (host) -> the context's dA0 (original) and dA (factors, in
+// the chosen precision), factors copied back into A.
+int factor_host_impl(lp_ctx* c, int precision, int n, int bs, float* A, int lda, lp_timing* t) {
+    c->fac_n = 0;
+    cudaStream_t st = c->stream;
+    const size_t abytes = sizeof(float) * (size_t)n * lda;
+    LP_CHECK(c->dA.ensure(abytes));
+    LP_CHECK(c->dA0.ensure(abytes));
+    float* dA = static_cast<float*>(c->dA.ptr);
+    float* dA0 = static_cast<float*>(c->dA0.ptr);
+    LP_CUDA(cudaEventRecord(c->ev[0], st));
+    LP_CUDA(cudaMemcpyAsync(dA0, A, abytes, cudaMemcpyHostToDevice, st));
+    LP_CUDA(cudaEventRecord(c->ev[1], st));
+    LP_CUDA(cudaMemcpyAsync(dA, dA0, abytes, cudaMemcpyDeviceToDevice, st));
+    LP_CUDA(cudaEventRecord(c->ev[2], st));
+    if (precision == LP_F32)
+        LP_CHECK(gefa_f32(c, dA, n, lda, bs, st));
+    else
+        LP_CHECK(gefa_mixed(c, precision, dA, n, lda, bs, st));
+    LP_CUDA(cudaEventRecord(c->ev[3], st));
+    LP_CUDA(cudaMemcpyAsync(A, dA, abytes, cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaEventRecord(c->ev[4], st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    c->fac_n = n;
+    c->fac_lda = lda;
+    c->fac_prec = precision;
+    if (t != nullptr) {
+        std::memset(t, 0, sizeof(*t));
+        t->h2d_s = ev_s(c->ev[0], c->ev[1]);
+        t->gefa_s = ev_s(c->ev[2], c->ev[3]);
+        t->d2h_s = ev_s(c->ev[3], c->ev[4]);
+    }
+    return LP_OK;
+}
+
+// lp_solve: B (host, FP32, nrhs rows of n) -> X (host, FP64) with the
+// resident factors; FP64 refinement against the original matrix for the
+// tensor-core precisions, none for LP_F32 (x = the FP32 solve widened).
+int solve_resident_impl(lp_ctx* c, int nrhs, const float* B, double* X, lp_timing* t) {
+    cudaStream_t st = c->stream;
+    const int n = c->fac_n, lda = c->fac_lda;
+    const size_t nv = (size_t)n * nrhs;
+    std::vector<double> b64(B, B + nv);  // FP32 right-hand sides widened exactly
+    LP_CHECK(c->dB64.ensure(sizeof(double) * nv));
+    LP_CHECK(c->dX.ensure(sizeof(double) * nv));
+    double* dB64 = static_cast<double*>(c->dB64.ptr);
+    double* dX = static_cast<double*>(c->dX.ptr);
+    LP_CUDA(cudaEventRecord(c->ev[0], st));
+    LP_CUDA(cudaMemcpyAsync(dB64, b64.data(), sizeof(double) * nv, cudaMemcpyHostToDevice, st));
+    LP_CUDA(cudaEventRecord(c->ev[1], st));
+    int iters = 0;
+    double resid = 0.0;
+    const int max_iters = c->fac_prec == LP_F32 ? 0 : kSolveMaxRefinements;
+    const int s = refine_core(c, static_cast<const float*>(c->dA0.ptr), lda, static_cast<const float*>(c->dA.ptr), n,
+                              dB64, dX, nrhs, max_iters, &iters, &resid, st);
+    LP_CUDA(cudaEventRecord(c->ev[5], st));
+    LP_CUDA(cudaMemcpyAsync(X, dX, sizeof(double) * nv, cudaMemcpyDeviceToHost, st));
+    LP_CUDA(cudaEventRecord(c->ev[6], st));
+    LP_CUDA(cudaStreamSynchronize(st));
+    if (t != nullptr) {
+        std::memset(t, 0, sizeof(*t));
+        t->h2d_s = ev_s(c->ev[0], c->ev[1]);
+        t->gesl_s = ev_s(c->ev[1], c->ev[4]);
         t->ir_s = ev_s(c->ev[4], c->ev[5]);
         t->d2h_s = ev_s(c->ev[5], c->ev[6]);
         t->ir_iters = iters;

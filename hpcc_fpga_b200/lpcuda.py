@@ -177,6 +177,8 @@ def lib() -> ctypes.CDLL:
     L.lp_gesl_pvt_dev.argtypes = [_VP, _VP, _I, _I, _VP, _VP, _I, _I]
     L.lp_calculate_pvt.argtypes = [_VP, _I, _I, _I, _F32P, _F32P, _I32P, _F64P, _F64P]
     L.lp_solve_host.argtypes = [_VP, _I, _I, _I, _F32P, _I, _F64P, _I, _F64P, _I, ctypes.POINTER(LpTiming)]
+    L.lp_factor.argtypes = [_VP, _I, _I, _I, _F32P, _I, ctypes.POINTER(LpTiming)]
+    L.lp_solve.argtypes = [_VP, _I, _I, _F32P, _F64P, ctypes.POINTER(LpTiming)]
     L.lp_batch_default_config.argtypes = [ctypes.POINTER(LpBatchConfig)]
     L.lp_batch_solve_dev.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig),
                                      ctypes.POINTER(LpBatchStats)]
@@ -417,6 +419,26 @@ class Context:
         check(lib().lp_solve_host(self._h, PRECISIONS[precision], n, bs, A, A.shape[1], B, nrhs, x, max_iters,
                                   ctypes.byref(t)), "lp_solve_host")
         return (x[0] if np.ndim(b64) == 1 else x), t.as_dict()
+
+    def factor(self, A: np.ndarray, bs: int, precision: str = "f32") -> dict:
+        """Factor the host matrix A in place (factors in the reference encoding
+        written back) and keep the factors resident for solve()."""
+        if A.dtype != np.float32 or not A.flags.c_contiguous:
+            raise ValueError("factor: A must be a C-contiguous float32 array (it is overwritten)")
+        t = LpTiming()
+        check(lib().lp_factor(self._h, PRECISIONS[precision], A.shape[0], bs, A, A.shape[1], ctypes.byref(t)),
+              "lp_factor")
+        return t.as_dict()
+
+    def solve(self, B: np.ndarray):
+        """Solve with the resident factors of the last factor(): B (n,) or
+        (nrhs, n) float32 -> (x float64 of the same shape, timing dict)."""
+        Bm = np.ascontiguousarray(np.atleast_2d(B), dtype=np.float32)
+        nrhs, n = Bm.shape
+        x = np.empty((nrhs, n), np.float64)
+        t = LpTiming()
+        check(lib().lp_solve(self._h, n, nrhs, Bm, x, ctypes.byref(t)), "lp_solve")
+        return (x[0] if np.ndim(B) == 1 else x), t.as_dict()
 
 
 # ------------------------------------------------------------------ pinned host memory

@@ -275,6 +275,29 @@ int lp_calculate_pvt(lp_ctx* ctx, int n, int lda, int repetitions, float* A, flo
 int lp_solve_host(lp_ctx* ctx, int precision, int n, int bs, float* A, int lda, const double* b64, int nrhs,
                   double* x, int max_iters, lp_timing* t);
 
+/* The two halves of lp_solve_host, with the factors resident in between, for
+ * callers that solve several right-hand sides against one matrix.
+ * lp_factor replaces the factorization half of execution::pcie::calculate:
+ * the block-row loop (execution_types/execution_pcie.hpp:177-641) and the
+ * copy of the factors back into data.A (:695-696).  It factors the host
+ * matrix A (n x n, leading dimension lda) in the chosen precision (bs as for
+ * lp_gefa_prec_dev), writes the factors back into A in the reference
+ * encoding, and keeps them and the original matrix in the context.
+ * t (optional): h2d_s, gefa_s, d2h_s. */
+int lp_factor(lp_ctx* ctx, int precision, int n, int bs, float* A, int lda, lp_timing* t);
+/* lp_solve replaces the host substitution after calculate
+ * (gesl_ref_nopvt, LINPACK/src/host/linpack_data.cpp:199-229, called at
+ * linpack_benchmark.hpp:321-323).  It solves with the factors of the last
+ * lp_factor on this context: B (nrhs rows of n floats, host) -> X (nrhs rows
+ * of n doubles, host).  LP_F32 factors: X is the FP32 substitution widened
+ * to double.  Tensor-core precisions: FP64 refinement against the original
+ * matrix until the HPL scaled residual is <= 16, at most 50 refinements.
+ * t (optional): h2d_s, gesl_s, ir_s, d2h_s, ir_iters, hpl_resid.
+ * LP_E_INVALID without resident factors or with another n.  lp_calculate,
+ * lp_calculate_pvt and lp_solve_host on the same context discard the
+ * resident factors. */
+int lp_solve(lp_ctx* ctx, int n, int nrhs, const float* B, double* X, lp_timing* t);
+
 /* ---- batched solves (addition: no counterpart in the reference) ------------
  * Many independent diagonally dominant systems (1 <= n <= 1024, 1 <= nrhs
  * <= 16) factored in place (reference encoding) and solved in ONE persistent

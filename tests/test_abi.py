@@ -34,6 +34,9 @@ def test_null_context_rejected(lp):
     assert L.lp_gefa_dev(None, None, 128, 128, 128) == lp.LP_E_INVALID
     assert L.lp_gesl_dev(None, None, 128, 128, None, 1, 128) == lp.LP_E_INVALID
     assert L.lp_ctx_sync(None) == lp.LP_E_INVALID
+    A = np.zeros((16, 16), np.float32)
+    assert L.lp_factor(None, 0, 16, 16, A, 16, None) == lp.LP_E_INVALID
+    assert L.lp_solve(None, 16, 1, np.zeros(16, np.float32), np.zeros(16), None) == lp.LP_E_INVALID
     assert "null" in lp.last_error()
     assert L.lp_ctx_destroy(None) == 0
 

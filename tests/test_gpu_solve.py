@@ -13,6 +13,7 @@ import oracle
 
 pytestmark = pytest.mark.gpu
 FLT_EPS = float(np.finfo(np.float32).eps)
+DBL_EPS = float(np.finfo(np.float64).eps)
 
 
 @pytest.mark.parametrize("bs", [16, 32, 128, 512])
@@ -125,6 +126,59 @@ def test_solve_host_f32_and_refined(ctx):
     assert oracle.hpl_resid(A, x2, b64) <= 16.0
     # Refinement stops at the HPL threshold, not at full FP64 accuracy.
     assert np.abs(x2 - 1.0).max() < 1e-10
+
+
+@pytest.mark.parametrize("prec", ["f32", "bf16", "fp8", "f32_bf16x6"])
+def test_factor_then_solve_matches_solve_host(ctx, dev, lp, prec):
+    """lp_factor + lp_solve (factors resident between the calls) give what
+    lp_solve_host gives in one call, on two solves against one factorization;
+    the factors written back equal the device factorization's."""
+    n, bs = 1024, 256
+    A, _, _ = oracle.gen_baseline(n, seed=42, margin=1.0)
+    Af = A.copy()
+    t = ctx.factor(Af, bs, prec)
+    assert t["gefa_s"] > 0
+    d = dev.put(A)
+    if prec == "f32":
+        ctx.gefa(d.data_ptr(), n, n, bs)
+    else:
+        ctx.gefa_prec(prec, d.data_ptr(), n, n, bs)
+    assert np.array_equal(Af, dev.get(d))
+    rng = np.random.default_rng(3)
+    refine = 0 if prec == "f32" else 50
+    with lp.Context(0) as other:
+        for rep in range(2):
+            B = rng.uniform(-1, 1, (2, n)).astype(np.float32)
+            x, ts = ctx.solve(B)
+            x_ref, _ = other.solve_host(A, B.astype(np.float64), bs, prec, max_iters=refine)
+            # the same arithmetic; refined solves may stop one refinement apart at the threshold
+            assert np.abs(x - x_ref).max() <= (1e-9 if refine else 1e-13) * np.abs(x_ref).max()
+            eps = DBL_EPS / 2 if refine else FLT_EPS / 2
+            for q in range(2):
+                assert oracle.hpl_resid(A, x[q], B[q].astype(np.float64), eps=eps) <= 16.0
+            if refine:
+                assert ts["hpl_resid"] <= 16.0
+
+
+def test_solve_needs_resident_factors(lp):
+    """lp_solve without factors, with another n, or after an entry point
+    that reuses the context's matrix workspace is rejected."""
+    n, bs = 256, 64
+    A, _, b32 = oracle.gen_baseline(n, seed=1, margin=1.0)
+    with lp.Context(0) as c:
+        with pytest.raises(lp.LpError) as e:
+            c.solve(b32)
+        assert e.value.status == lp.LP_E_INVALID
+        c.factor(A.copy(), bs)
+        x, _ = c.solve(b32)
+        assert np.abs(x - 1.0).max() < 1e-3
+        with pytest.raises(lp.LpError) as e:
+            c.solve(np.ones(n - 64, np.float32))
+        assert e.value.status == lp.LP_E_INVALID
+        c.solve_host(A, b32.astype(np.float64), bs, "f32")
+        with pytest.raises(lp.LpError) as e:
+            c.solve(b32)
+        assert e.value.status == lp.LP_E_INVALID
 
 
 def test_non_dominant_matrix_reports_numeric_error(ctx, lp):
