@@ -119,14 +119,15 @@ __device__ __forceinline__ void split3(float x, __nv_bfloat16& a, __nv_bfloat16&
 // Segment s of the K = nseg k operand pairs L-term lterm(s) with T-term
 // tterm(s) (term 0 = x1, the largest).  nseg 6: x3 t1 + x2 t2 + x1 t3 +
 // x2 t1 + x1 t2 + x1 t1 (FP32 accuracy); nseg 3: x2 t1 + x1 t2 + x1 t1
-// (about 2^-16 relative, the three-term split's first two terms).
+// (about 2^-16 relative, the three-term split's first two terms); nseg 1:
+// x1 t1 (plain BF16 operands).
 template <int NSEG>
 __host__ __device__ constexpr int lterm(int s) {
-    return NSEG == 6 ? (s == 0 ? 2 : (s == 1 || s == 3) ? 1 : 0) : (s == 0 ? 1 : 0);
+    return NSEG == 6 ? (s == 0 ? 2 : (s == 1 || s == 3) ? 1 : 0) : NSEG == 3 ? (s == 0 ? 1 : 0) : 0;
 }
 template <int NSEG>
 __host__ __device__ constexpr int tterm(int s) {
-    return NSEG == 6 ? (s == 2 ? 2 : (s == 1 || s == 4) ? 1 : 0) : (s == 1 ? 1 : 0);
+    return NSEG == 6 ? (s == 2 ? 2 : (s == 1 || s == 4) ? 1 : 0) : NSEG == 3 ? (s == 1 ? 1 : 0) : 0;
 }
 
 // out[r][s*k + c] = term lterm(s) of L[r][c]: rows x (NSEG k) BF16.
@@ -190,12 +191,12 @@ __global__ void k_eye2(float* __restrict__ x, float* __restrict__ y, int n) {
 
 }  // namespace
 
-// The split-BF16 operands of a block step (nseg 6 or 3 K-segments):
+// The split-BF16 operands of a block step (nseg 6, 3 or 1 K-segments):
 // aq: rows_l x nseg k, bq: cols_t x nseg k.
 int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
                 uint8_t* bq, cudaStream_t st, int nseg) {
     if (rows_l <= 0 || cols_t <= 0) return LP_OK;
-    if (nseg != 6 && nseg != 3) return fail(LP_E_INVALID, "split_panel: 3 or 6 segments");
+    if (nseg != 6 && nseg != 3 && nseg != 1) return fail(LP_E_INVALID, "split_panel: 1, 3 or 6 segments");
     const size_t total = (size_t)rows_l * k;
     const int grid = (int)((total + 255) / 256 < 4736 ? (total + 255) / 256 : 4736);
     const dim3 tgrid((cols_t + 31) / 32, (k + 31) / 32);
@@ -204,9 +205,12 @@ int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, in
     if (nseg == 6) {
         k_split_rows<6><<<grid, 256, 0, st>>>(L, ldl, a, rows_l, k);
         k_split_trans<6><<<tgrid, 256, 0, st>>>(T, ldt, b, k, cols_t);
-    } else {
+    } else if (nseg == 3) {
         k_split_rows<3><<<grid, 256, 0, st>>>(L, ldl, a, rows_l, k);
         k_split_trans<3><<<tgrid, 256, 0, st>>>(T, ldt, b, k, cols_t);
+    } else {
+        k_split_rows<1><<<grid, 256, 0, st>>>(L, ldl, a, rows_l, k);
+        k_split_trans<1><<<tgrid, 256, 0, st>>>(T, ldt, b, k, cols_t);
     }
     count_launch(2);
     LP_CUDA(cudaGetLastError());
@@ -333,9 +337,14 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     LP_CHECK(c->q.ensure(4 * esz * pan));
     LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)nblk));
     LP_CHECK(c->err.ensure(sizeof(int)));
-    // the top / left products: FP32 accuracy for the emulated-FP32 form, three
-    // segments where the panel is rounded to BF16 / E4M3 afterwards anyway
-    const int nseg = x6 ? 6 : 3;
+    // the top / left products: FP32 accuracy (six segments) for the emulated-FP32
+    // form.  For BF16 / E4M3 (the panel is rounded to them for the update anyway)
+    // three segments, and plain BF16 operands from block 2048 on, where the panel
+    // chain is the critical path: the products cost about 9 bs / n of the update's
+    // flops per three segments.  Measured on one B200 (BF16+IR): n = 65536, block
+    // 2048: 582 -> 638 TFLOP/s, one refinement either way; n = 32768, block 1024: no
+    // gain, the plainer factors needing a second refinement.
+    const int nseg = x6 ? 6 : bs >= 2048 ? 1 : 3;
     LP_CHECK(c->tri.ensure(3 * sizeof(float) * (size_t)bs * bs));
     LP_CHECK(c->tq.ensure(2 * sizeof(__nv_bfloat16) * (size_t)nseg * bs * ((size_t)bs + n)));
     LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
