@@ -1,8 +1,8 @@
 #!/usr/bin/env python
-"""LINPACK LU + solve on B200 — prints ONE JSON line.
+"""LINPACK LU + solve on B200 — prints ONE compact JSON line.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl lpcuda|reference]
-                    [--n 32768] [--bs 512]
+                    [--n 32768] [--bs 512] [--details PATH]
 
 A step is one factorization (blocked LU without pivoting, the reference's
 lu/top/left/inner stages) plus forward/back substitution of one n x n system
@@ -16,6 +16,13 @@ execution::pcie::calculate) with pinned host buffers: host->device copy of A
 and b, factor, solve, device->host copy of the factors and x, all inside the
 wall-clock timed call.
 
+Beside the headline the run measures the mixed-precision forms (BF16 / FP8
+E4M3 trailing updates + FP64 refinement) with the diagonal-dominance margin
+swept over {1, 0.1 sqrt(n), n} at n = 32768 and n = 65536, the emulated-FP32,
+pivoting and FP64 paths, the batched solver and the serving loop.  The last
+stdout line is a compact summary of a few KB; every table in full goes to the
+JSON file named by --details.
+
 Multi-GPU: the path does not shard (one system per GPU); under torchrun each
 rank runs an independent replica, time = max over ranks, value = total work
 of all ranks / that time.
@@ -25,6 +32,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -41,10 +49,17 @@ METRIC = "LU+solve GFLOP/s FP32 vs BF16/FP8+IR at equal residual; batched solves
 UNIT = "GFLOP/s"
 NUM_SMS = 148
 FP32_LANES_PER_SM = 128
+FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
+LINE_LIMIT = 2600  # bytes: the summary line must survive a few-KB stdout tail whole
 
 
 def flops(n: int) -> float:
     return 2.0 * n ** 3 / 3.0 + 2.0 * n ** 2
+
+
+def margins_for(n: int) -> list:
+    """The diagonal-dominance margins of the mixed-precision sweep: 1, 0.1 sqrt(n), n."""
+    return [1.0, 0.1 * math.sqrt(n), float(n)]
 
 
 def peaks() -> dict:
@@ -56,6 +71,17 @@ def peaks() -> dict:
         return d
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "sm_max_mhz": 1965.0,
             "source": "fallback"}
+
+
+def host_cpu() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 class ClockSampler:
@@ -105,22 +131,40 @@ class ClockSampler:
                 "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
 
 
-def cpu_baseline(n: int, reps: int) -> dict:
+class CpuBaseline:
     """The reference's own gefa_ref_nopvt + gesl_ref_nopvt (compiled from
     LINPACK/src/host/linpack_data.cpp into oracle/_ref/ref_bench), timed on
-    this host, on a bounded sample of the workload (same generator)."""
-    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
-    if not os.path.exists(exe):
-        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/ref_bench not built"}
-    out = subprocess.run([exe, "--n", str(n), "--reps", str(reps), "--mode", "baseline", "--seed", "42",
-                          "--margin", "1"], capture_output=True, text=True, check=True).stdout
-    r = json.loads(out.strip().splitlines()[-1])
-    return {"value": r["gflops"], "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"one n={n} system (seed 42, margin 1), best of {reps}: gefa_ref_nopvt+gesl_ref_nopvt, "
-                      f"single-threaded reference code, g++ -O3 -march=x86-64-v3; "
-                      f"residual_norm {r['residual_norm']:.3g}",
-            "t_min_s": r["t_min"], "host_nproc": os.cpu_count()}
+    one host core on the configured sample (same seeded generator).  The
+    reference code is serial, so it runs as a background process on one core
+    while the GPU legs run, and is collected before the serving leg (whose
+    worker threads want the host cores)."""
+
+    def __init__(self, n: int, reps: int):
+        self.n, self.reps = n, reps
+        self.exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+        self.proc = None
+        self.t0 = time.perf_counter()
+        if os.path.exists(self.exe):
+            self.proc = subprocess.Popen([self.exe, "--n", str(n), "--reps", str(reps), "--mode", "baseline",
+                                          "--seed", "42", "--margin", "1"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.PIPE, text=True)
+
+    def result(self) -> dict:
+        if self.proc is None:
+            return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                    "sample": "unavailable: oracle/_ref/ref_bench not built"}
+        out, err = self.proc.communicate()
+        if self.proc.returncode != 0:
+            return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                    "sample": f"ref_bench failed ({self.proc.returncode}): {err.strip()[:200]}"}
+        r = json.loads(out.strip().splitlines()[-1])
+        return {"value": r["gflops"], "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": f"one n={self.n} system (seed 42, margin 1), best of {self.reps}: gefa_ref_nopvt + "
+                          "gesl_ref_nopvt compiled from the reference sources (g++ -O3 -march=x86-64-v3), "
+                          "serial code on one core",
+                "n": self.n, "t_min_s": r["t_min"], "gflops_lu": r["gflops_lu"], "residual_norm": r["residual_norm"],
+                "host_nproc": os.cpu_count(), "host_cpu": host_cpu(),
+                "wall_s": round(time.perf_counter() - self.t0, 1)}
 
 
 def mixed_block(n: int, bs: int) -> int:
@@ -136,21 +180,9 @@ def mixed_block(n: int, bs: int) -> int:
     return max(bs, b)
 
 
-def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, f32_value, pk) -> dict:
-    """BF16 / FP8 trailing updates + FP64 refinement to the HPL threshold on
-    the same system: GFLOP/s by the same formula over factor + all solves +
-    refinement (the refinement's own 2n^2 flop per iteration not credited)."""
-    with torch.cuda.stream(stream):
-        dB64 = torch.from_numpy(b64).to("cuda")
-        dX = torch.empty(n, dtype=torch.float64, device="cuda")
-    info = {}
-
-    def step():
-        with torch.cuda.stream(stream):
-            dA.copy_(dA0)
-        ctx.gefa_prec(prec, dA.data_ptr(), n, n, bs)
-        info.update(ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dX.data_ptr(), 1, 50))
-
+def timed_steps(torch, ctx, stream, step, steps: int, warmup: int):
+    """warmup untimed steps, then `steps` steps between two CUDA events on the
+    library's stream, with the stage profile of the timed steps."""
     for _ in range(warmup):
         step()
     ctx.sync()
@@ -160,25 +192,50 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, 
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    iters = []
-    resid = []
-    for _ in range(steps):
-        step()
-        iters.append(info["ir_iters"])
-        resid.append(info["hpl_resid"])
+    out = [step() for _ in range(steps)]
     ev1.record(stream)
     torch.cuda.synchronize()
-    t = ev0.elapsed_time(ev1) * 1e-3
     prof = ctx.read_profile(reset=True)
     ctx.set_profiling(False)
-    x = dX.cpu().numpy()
-    # GMRES-based refinement (gmres_ref on the device) on the same factors, from x = 0
+    return ev0.elapsed_time(ev1) * 1e-3, prof, out
+
+
+def run_f32(ctx, lp, torch, stream, dA0, dA, dB0, dB, n, bs, steps, warmup) -> dict:
+    """The plain FP32 step on one system: restore A and b, factor, solve."""
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+            dB.copy_(dB0)
+        ctx.gefa(dA.data_ptr(), n, n, bs)
+        ctx.gesl(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
+
+    t, prof, _ = timed_steps(torch, ctx, stream, step, steps, warmup)
+    inner = prof["inner"]
+    return {"n": n, "block": bs, "value": steps * flops(n) / t / 1e9, "ms_per_step": 1e3 * t / steps,
+            "inner_tflops": inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None,
+            "max_abs_err_x": float((dB.double() - 1.0).abs().max()),
+            "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]}}
+
+
+def run_mixed(ctx, lp, torch, stream, dA0, dA, dB64, n, bs, prec, steps, warmup, f32_value, pk,
+              with_gmres: bool = True) -> dict:
+    """BF16 / FP8 trailing updates + FP64 refinement to the HPL threshold on
+    the system in dA0 (right-hand side dB64, exact solution all ones): GFLOP/s
+    by the same formula over factor + all solves + refinement (the
+    refinement's own 2n^2 flop per iteration not credited)."""
     with torch.cuda.stream(stream):
-        dXg = torch.zeros(n, dtype=torch.float64, device="cuda")
-    g = ctx.gmres(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dXg.data_ptr(), 50, 3, 1e-12)
-    gmres = {"seconds": g["ir_s"], "arnoldi_steps": g["ir_iters"], "hpl_resid": g["hpl_resid"],
-             "max_abs_err_vs_fp64_oracle": float((dXg - 1.0).abs().max()),
-             "note": "restart 50, 3 cycles, tol 1e-12, preconditioner = these factors applied in FP64"}
+        dX = torch.empty(n, dtype=torch.float64, device="cuda")
+    info = {}
+
+    def step():
+        with torch.cuda.stream(stream):
+            dA.copy_(dA0)
+        ctx.gefa_prec(prec, dA.data_ptr(), n, n, bs)
+        info.update(ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dX.data_ptr(), 1, 50))
+        return info["ir_iters"], info["hpl_resid"]
+
+    t, prof, res = timed_steps(torch, ctx, stream, step, steps, warmup)
+    err = float((dX - 1.0).abs().max())
     inner = prof["inner"]
     gbs = inner["bytes"] / inner["s"] / 1e9 if inner["s"] > 0 else None
     tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
@@ -190,10 +247,12 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, 
     tpk = pk["bf16_tflops"] * (2.0 if prec == "fp8" else 1.0)
     ridge = tpk * 1e12 / (pk["hbm_gbs"] * 1e9)
     tensor_bound = bs / 4.0 > ridge
-    return {
-        "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32": value / f32_value,
-        "ir_iters": max(iters), "hpl_resid": max(resid), "hpl_eps": "DBL_EPSILON/2",
-        "max_abs_err_vs_fp64_oracle": float(np.abs(x - 1.0).max()),
+    out = {
+        "n": n, "block": bs, "precision": prec,
+        "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps,
+        "speedup_vs_f32": value / f32_value if f32_value else None,
+        "ir_iters": max(r[0] for r in res), "hpl_resid": max(r[1] for r in res), "hpl_eps": "DBL_EPSILON/2",
+        "max_abs_err_vs_fp64_oracle": err,
         "roofline": {"bound": "tensor" if tensor_bound else "hbm",
                      "kernel": f"k_umma_update<{prec}> (inner stage, tcgen05)",
                      "achieved": tfs if tensor_bound else gbs,
@@ -204,15 +263,61 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, bs, prec, steps, warmup, 
                      "tensor_frac": tfs / tpk if tfs else None,
                      "per_unit": f"8*m*n bytes (FP32 C read+write) and 2*m*n*{bs} flop per m x n trailing "
                                  f"update: intensity {bs / 4:.0f} flop/B against the {prec} ridge {ridge:.0f} flop/B",
-                     "tensor_tflops": tfs, "tensor_peak_tflops": tpk,
                      "peak_source": pk["source"] + ("; FP8 peak = 2 x the measured BF16 rate" if prec == "fp8"
                                                     else "")},
         "stages": {k: {"s": prof[k]["s"], "calls": prof[k]["calls"]} for k in lp.STAGES if prof[k]["calls"]},
-        "gmres": gmres,
     }
+    if with_gmres:
+        # GMRES-based refinement (gmres_ref on the device) on the same factors, from x = 0
+        with torch.cuda.stream(stream):
+            dXg = torch.zeros(n, dtype=torch.float64, device="cuda")
+        g = ctx.gmres(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dXg.data_ptr(), 50, 3, 1e-12)
+        out["gmres"] = {"seconds": g["ir_s"], "arnoldi_steps": g["ir_iters"], "hpl_resid": g["hpl_resid"],
+                        "max_abs_err_vs_fp64_oracle": float((dXg - 1.0).abs().max()),
+                        "note": "restart 50, 3 cycles, tol 1e-12, preconditioner = these factors applied in FP64"}
+    return out
 
 
-def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, steps, warmup, f32_value, pk) -> dict:
+def run_margin_sweep(ctx, lp, torch, stream, dA0, dA, n, bs, precs, steps, warmup, f32_value, pk,
+                     skip_margin_one: dict | None = None) -> list:
+    """The mixed-precision forms over the margins {1, 0.1 sqrt(n), n} of the
+    seeded generator: the diagonal (and b64) of dA0 are rewritten on the
+    device per margin — bit-identical to drawing the matrix again with that
+    margin — and restored to margin 1 afterwards.  Per case: IR iterations,
+    HPL scaled residual and max |x - 1| (the FP64 oracle's solution is exactly
+    all ones)."""
+    from hpcc_fpga_b200.workload import set_margin
+
+    rows = []
+    diag1 = dA0.diagonal().clone()
+    try:
+        for m in margins_for(n):
+            if m == 1.0 and skip_margin_one:
+                for prec in precs:
+                    r = skip_margin_one.get(prec)
+                    if r is not None:
+                        rows.append({"n": n, "precision": prec, "block": bs, "margin": m, "value": r["value"],
+                                     "ir_iters": r["ir_iters"], "hpl_resid": r["hpl_resid"],
+                                     "max_abs_err": r["max_abs_err_vs_fp64_oracle"]})
+                continue
+            with torch.cuda.stream(stream):
+                dB64 = set_margin(torch, dA0, n, m)
+            torch.cuda.synchronize()
+            for prec in precs:
+                r = run_mixed(ctx, lp, torch, stream, dA0, dA, dB64, n, bs, prec, steps, warmup, f32_value, pk,
+                              with_gmres=False)
+                rows.append({"n": n, "precision": prec, "block": bs, "margin": m, "value": r["value"],
+                             "ir_iters": r["ir_iters"], "hpl_resid": r["hpl_resid"],
+                             "max_abs_err": r["max_abs_err_vs_fp64_oracle"]})
+            del dB64
+    finally:
+        with torch.cuda.stream(stream):
+            dA0.diagonal().copy_(diag1)
+        torch.cuda.synchronize()
+    return rows
+
+
+def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, dB64, n, bs, steps, warmup, f32_value, pk) -> dict:
     """FP32 emulated on the BF16 tensor cores (LP_F32_BF16X6: exact three-term
     BF16 split of every operand, six products, FP32 accumulation) on the same
     system and the same step as the FP32 headline: restore A and b, factor,
@@ -224,43 +329,27 @@ def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, bs, steps, warm
         ctx.gefa_prec("f32_bf16x6", dA.data_ptr(), n, n, bs)
         ctx.gesl(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
 
-    for _ in range(warmup):
-        step()
-    ctx.sync()
-    ctx.set_profiling(True)
-    ctx.read_profile(reset=True)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t = ev0.elapsed_time(ev1) * 1e-3
-    prof = ctx.read_profile(reset=True)
-    ctx.set_profiling(False)
-    x = dB.cpu().numpy().astype(np.float64)
+    t, prof, _ = timed_steps(torch, ctx, stream, step, steps, warmup)
+    err = float((dB.double() - 1.0).abs().max())
     with torch.cuda.stream(stream):
-        dB64 = torch.from_numpy(b64).to("cuda")
         dXr = torch.empty(n, dtype=torch.float64, device="cuda")
     r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
     inner = prof["inner"]
     tf32eq = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
     value = steps * flops(n) / t / 1e9
+    spk = pk.get("bf16_tflops_sustained", pk["bf16_tflops"])
     return {
         "workload": f"the FP32 workload's system and step (n={n}) in blocks of {bs}, with the trailing update "
                     "and the panel's top/left products emulated on the BF16 tensor cores: exact 3-term BF16 split, "
                     "6 products, FP32 accumulation; plain FP32 solve, no refinement",
         "block": bs,
         "value": value, "unit": UNIT, "ms_per_step": 1e3 * t / steps, "speedup_vs_f32_simt": value / f32_value,
-        "max_abs_err_x": float(np.abs(x - 1.0).max()),
+        "max_abs_err_x": err,
         "hpl_resid": {"eps_flt_half": r32 * 2.0 ** -29, "eps_dbl_half": r32},
         # timed inside a seconds-long factorization: the sustained BF16 figure is the denominator
         "roofline": {"bound": "tensor", "kernel": "k_umma_update (inner stage, K = 6 bs)",
-                     "achieved": 6 * tf32eq if tf32eq else None,
-                     "peak": pk.get("bf16_tflops_sustained", pk["bf16_tflops"]), "unit": "TFLOP/s",
-                     "frac": 6 * tf32eq / pk.get("bf16_tflops_sustained", pk["bf16_tflops"]) if tf32eq else None,
+                     "achieved": 6 * tf32eq if tf32eq else None, "peak": spk, "unit": "TFLOP/s",
+                     "frac": 6 * tf32eq / spk if tf32eq else None,
                      "fp32_equivalent_tflops": tf32eq,
                      "peak_source": pk["source"] + " (bf16_tflops_sustained; burst " + str(pk["bf16_tflops"]) + ")",
                      "per_unit": "6 x 2*m*n*bs BF16 flop per m x n trailing update (2*m*n*bs FP32-equivalent)"},
@@ -336,46 +425,27 @@ def run_batched(ctx, lp, torch, stream, steps, warmup, count=4096) -> dict:
     }
 
 
-FLT_EPS_HALF = float(np.finfo(np.float32).eps) / 2
-
-
-def run_fp64(ctx, lp, torch, stream, A, b64, n, steps, warmup, peak_fp64) -> dict:
+def run_fp64(ctx, lp, torch, stream, dA32, db64, n, steps, warmup, peak_fp64) -> dict:
     """The double build (DATA_TYPE double): the same system's FP32 entries
     widened to double, b in double (x = ones exactly); a step = restore A,
     lp_gefa_f64_dev (bs 256) + lp_gesl_f64_dev, on device time."""
     bs = 256
     with torch.cuda.stream(stream):
-        dA0 = torch.from_numpy(A).to("cuda").double()
-        db0 = torch.from_numpy(b64).to("cuda")
+        dA0 = dA32.double()
         dA = torch.empty_like(dA0)
-        dB = torch.empty_like(db0)
+        dB = torch.empty_like(db64)
     torch.cuda.synchronize()
 
     def step():
         with torch.cuda.stream(stream):
             dA.copy_(dA0)
-            dB.copy_(db0)
+            dB.copy_(db64)
         ctx.gefa_f64(dA.data_ptr(), n, n, bs)
         ctx.gesl_f64(dA.data_ptr(), n, n, dB.data_ptr(), 1, n)
 
-    for _ in range(warmup):
-        step()
-    ctx.sync()
-    ctx.set_profiling(True)
-    ctx.read_profile(reset=True)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t = ev0.elapsed_time(ev1) * 1e-3
-    prof = ctx.read_profile(reset=True)
-    ctx.set_profiling(False)
+    t, prof, _ = timed_steps(torch, ctx, stream, step, steps, warmup)
     resid = float((dB - 1.0).abs().max())
-    normb = float(db0.abs().max())
+    normb = float(db64.abs().max())
     inner = prof["inner"]
     tfs = inner["flops"] / inner["s"] / 1e12 if inner["s"] > 0 else None
     stage_s = {k: prof[k]["s"] for k in lp.STAGES if prof[k]["calls"]}
@@ -394,7 +464,7 @@ def run_fp64(ctx, lp, torch, stream, A, b64, n, steps, warmup, peak_fp64) -> dic
     }
 
 
-def run_pivot(ctx, lp, torch, stream, n, steps, warmup, pk) -> dict:
+def run_pivot(ctx, lp, torch, stream, n, steps, warmup, peak_tf) -> dict:
     """LU with partial pivoting (the harness's --uniform case, gefa_ref /
     gesl_ref convention) on a non-dominant matrix: U(0,1) entries (seed 42,
     torch's device generator), b = column sums of the storage (x = ones).
@@ -419,22 +489,7 @@ def run_pivot(ctx, lp, torch, stream, n, steps, warmup, pk) -> dict:
         ctx.gefa_pvt(dA.data_ptr(), n, n, dP.data_ptr())
         ctx.gesl_pvt(dA.data_ptr(), n, n, dP.data_ptr(), dB.data_ptr(), 1, n)
 
-    for _ in range(warmup):
-        step()
-    ctx.sync()
-    ctx.set_profiling(True)
-    ctx.read_profile(reset=True)
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(steps):
-        step()
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    t = ev0.elapsed_time(ev1) * 1e-3
-    prof = ctx.read_profile(reset=True)
-    ctx.set_profiling(False)
+    t, prof, _ = timed_steps(torch, ctx, stream, step, steps, warmup)
     x = dB.double()
     resid = float((x - 1.0).abs().max())
     normb = float(db0.max())
@@ -450,13 +505,39 @@ def run_pivot(ctx, lp, torch, stream, n, steps, warmup, pk) -> dict:
         "row_exchanges": swaps, "max_abs_err_x": resid,
         "residn": resid / (n * normb * float(np.finfo(np.float32).eps)),
         "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)", "achieved": tfs,
-                     "unit": "TFLOP/s"},
+                     "peak": peak_tf, "unit": "TFLOP/s", "frac": tfs / peak_tf if tfs else None},
         "stages": {k: {"s": v, "share": v / tot if tot > 0 else None, "calls": prof[k]["calls"]}
                    for k, v in stage_s.items()},
         "stage_names": {"lu": "k_piv_panel (pivot search, exchange, panel update)",
                         "left": "k_piv_rows (interchanges + triangular solve of the block row)",
                         "inner": "k_sgemm_update", "gesl": "k_piv_gesl"},
     }
+
+
+def run_gesl_noalloc(lp, torch, stream, dLU, dB0, n, steps) -> dict:
+    """lp_gesl_dev_noalloc (the allocation-free substitution: one launch per
+    128-row block and direction, k_gesl_fwd / k_gesl_bwd) on the factors of
+    the FP32 run, one right-hand side; device time per solve."""
+    dB = torch.empty_like(dB0)
+    L = lp.lib()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    secs = 0.0
+    for i in range(1 + steps):
+        with torch.cuda.stream(stream):
+            dB.copy_(dB0)
+            ev0.record(stream)
+        lp.check(L.lp_gesl_dev_noalloc(dLU.data_ptr(), n, n, dB.data_ptr(), 1, n, ctypes.c_void_p(stream.cuda_stream)),
+                 "lp_gesl_dev_noalloc")
+        with torch.cuda.stream(stream):
+            ev1.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:
+            secs += ev0.elapsed_time(ev1) * 1e-3
+    s = secs / steps
+    return {"kernels": "k_gesl_fwd / k_gesl_bwd (one launch per 128-row block and direction)",
+            "s_per_solve": s, "GBps": 4.0 * n * n / s / 1e9,
+            "max_abs_err_x": float((dB.double() - 1.0).abs().max())}
 
 
 RESERVE = 110 * 10 ** 9  # pool mapped at start: the 80 GB budget plus headroom against fragmentation
@@ -493,10 +574,133 @@ def run_serving(lp, rates, precisions, master_n=8192) -> dict:
     return out
 
 
+# ---------------------------------------------------------------- the summary line
+def sig(x, d: int = 4):
+    """x rounded to d significant digits; None for missing or non-finite values."""
+    if x is None:
+        return None
+    if isinstance(x, bool):
+        return x
+    if isinstance(x, int):
+        return x
+    try:
+        xf = float(x)
+    except (TypeError, ValueError):
+        return x
+    if not math.isfinite(xf):
+        return None
+    if xf == 0.0:
+        return 0.0
+    return float(f"{xf:.{d}g}")
+
+
+def _mixed_summary(r: dict | None) -> dict | None:
+    if not r:
+        return None
+    return {"value": sig(r.get("value")), "x_f32": sig(r.get("speedup_vs_f32"), 3), "iters": r.get("ir_iters"),
+            "hpl": sig(r.get("hpl_resid"), 3), "err": sig(r.get("max_abs_err_vs_fp64_oracle"), 2),
+            "frac": sig((r.get("roofline") or {}).get("frac"), 3)}
+
+
+def compact_line(full: dict) -> dict:
+    """The stdout summary: the contract's keys, the headline roofline, e2e,
+    CPU baseline and clocks, and one flat summary per extension.  Strict JSON
+    (no NaN / infinity) and at most LINE_LIMIT bytes; the full tables stay in
+    the details file."""
+    line = {k: full.get(k) for k in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                                     "higher_is_better", "scaling", "vs_baseline", "dtype", "data")}
+    for k in ("value", "ms_per_step"):
+        line[k] = sig(line[k], 6)
+    line["config"] = full.get("config")
+    rl = full.get("roofline") or {}
+    line["roofline"] = {"bound": rl.get("bound"), "achieved": sig(rl.get("achieved")), "peak": sig(rl.get("peak")),
+                        "unit": rl.get("unit"), "frac": sig(rl.get("frac"), 3), "traffic": sig(rl.get("traffic")),
+                        "kernel": "k_sgemm_update", "peak_src": rl.get("peak_short")}
+    e = full.get("e2e")
+    if e:
+        line["e2e"] = {"value": sig(e.get("value"), 6), "unit": e.get("unit"),
+                       "h2d_bytes_per_step": e.get("h2d_bytes_per_step"),
+                       "d2h_bytes_per_step": e.get("d2h_bytes_per_step"), "ms_per_step": sig(e.get("ms_per_step"))}
+    c = full.get("cpu_baseline")
+    if c:
+        line["cpu_baseline"] = {"value": sig(c.get("value")), "unit": c.get("unit"), "cores": c.get("cores"),
+                                "kind": c.get("kind"),
+                                "sample": f"n={c.get('n')} gefa_ref_nopvt+gesl_ref_nopvt, serial, 1 of "
+                                          f"{c.get('host_nproc')} cores"
+                                if c.get("value") else c.get("sample")}
+    ck = full.get("clocks") or {}
+    line["clocks"] = {"sm_mhz": ck.get("sm_mhz"), "sm_max_mhz": ck.get("sm_max_mhz"), "reasons": ck.get("reasons")}
+    line["gpu_launches"] = full.get("gpu_launches")
+    line["accuracy"] = {"max_abs_err_x": sig(full.get("max_abs_err_x"), 3),
+                        "hpl_resid_flt": sig((full.get("hpl_resid") or {}).get("eps_flt_half"), 3)}
+    g = full.get("gesl") or {}
+    line["gesl"] = {"GBps": sig(g.get("GBps")), "frac": sig(g.get("frac_hbm"), 3)}
+    if full.get("gesl_noalloc"):
+        line["gesl"]["noalloc_GBps"] = sig(full["gesl_noalloc"].get("GBps"))
+    mx = full.get("mixed") or {}
+    if mx:
+        first = next(iter(mx.values()))
+        line["mixed"] = {"n": first.get("n"), "block": first.get("block")}
+        line["mixed"].update({p: _mixed_summary(mx.get(p)) for p in ("bf16", "fp8") if mx.get(p)})
+    lg = full.get("large")
+    if lg:
+        f = lg.get("f32") or {}
+        line["large"] = {"n": lg.get("n"), "block": (lg.get("bf16") or lg.get("fp8") or {}).get("block"),
+                         "f32": sig(f.get("value")), "f32_frac": sig(f.get("frac"), 3)}
+        for p in ("bf16", "fp8"):
+            if lg.get(p):
+                line["large"][p] = _mixed_summary(lg[p])
+    ms = full.get("margins")
+    if ms:
+        rows = {}
+        for r in ms:
+            rows.setdefault(f"{r['n']} {r['precision']}", []).append(
+                [sig(r["margin"], 3), r["ir_iters"], sig(r["hpl_resid"], 3), sig(r["max_abs_err"], 2)])
+        line["margins"] = {"cols": ["margin", "iters", "hpl", "err"], **rows}
+    em = full.get("f32_bf16x6")
+    if em:
+        line["f32_bf16x6"] = {"value": sig(em.get("value")), "x_f32": sig(em.get("speedup_vs_f32_simt"), 3),
+                              "frac": sig((em.get("roofline") or {}).get("frac"), 3),
+                              "err": sig(em.get("max_abs_err_x"), 2)}
+    for key in ("pivot", "fp64"):
+        v = full.get(key)
+        if v:
+            line[key] = {"value": sig(v.get("value")), "frac": sig((v.get("roofline") or {}).get("frac"), 3)}
+    bt = full.get("batched")
+    if bt:
+        line["batched"] = {"solves_per_s": sig(bt.get("solves_per_s")), "value": sig(bt.get("value")),
+                           "x_loop": sig(bt.get("speedup_vs_per_system_loop_wall"), 3),
+                           "resid_max": sig(bt.get("hpl_resid_flt_eps_max_sample"), 3)}
+        for p in ("bf16",):
+            if bt.get(p):
+                line["batched"][p] = {"solves_per_s": sig(bt[p].get("solves_per_s")), "value": sig(bt[p].get("value")),
+                                      "iters": bt[p].get("ir_iters_max"), "resid_max": sig(bt[p].get("hpl_resid_max"), 3)}
+        if bt.get("frac") is not None:
+            line["batched"]["frac"] = sig(bt.get("frac"), 3)
+        if bt.get("speedup_vs_full_gpu_loop") is not None:
+            line["batched"]["x_full_gpu_loop"] = sig(bt.get("speedup_vs_full_gpu_loop"), 3)
+    sv = full.get("serving")
+    if sv:
+        line["serving"] = {}
+        for p in ("f32", "bf16", "fp8"):
+            eq = (sv.get(p) or {}).get("equal_p99")
+            if eq:
+                line["serving"][p] = {"x_equal_p99": eq.get("ratio"), "p99_ms": sig(eq.get("p99_bound_ms"), 3),
+                                      "solves_per_s": eq.get("continuous_solves_per_s"),
+                                      "base": eq.get("baseline_solves_per_s")}
+    if full.get("details"):
+        line["details"] = full["details"]
+    return line
+
+
+def dumps_line(line: dict) -> str:
+    return json.dumps(line, allow_nan=False, separators=(",", ":"))
+
+
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    n = args.cpu_n
+    n = args.ref_n
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
     if not os.path.exists(exe):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_bench not built"}))
@@ -519,7 +723,8 @@ def run_reference(args, rank: int) -> None:
                    "n": n, "sample_of_n": args.n, "block": args.bs},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
                          "sample": f"{args.steps} x one n={n} system; the reference's gefa_ref_nopvt/gesl_ref_nopvt "
-                                   "are single-threaded (no OpenMP in linpack_data.cpp), so one core is all they use"},
+                                   "are single-threaded (no OpenMP in linpack_data.cpp), so one core is all they use; "
+                                   f"host {host_cpu()}, {os.cpu_count()} cores"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -533,11 +738,19 @@ def main() -> None:
     ap.add_argument("--impl", default="lpcuda", choices=["lpcuda", "reference"])
     ap.add_argument("--n", type=int, default=32768)
     ap.add_argument("--bs", type=int, default=512)
-    ap.add_argument("--cpu-n", type=int, default=2048)
-    ap.add_argument("--cpu-reps", type=int, default=3)
+    ap.add_argument("--large-n", type=int, default=65536,
+                    help="order of the second system (FP32 and the mixed forms with their margin sweep); 0: skip")
+    ap.add_argument("--cpu-n", type=int, default=8192, help="order of the CPU-baseline sample (reference code)")
+    ap.add_argument("--cpu-reps", type=int, default=1)
+    ap.add_argument("--ref-n", type=int, default=2048, help="order of each step of the --impl reference arm")
+    ap.add_argument("--ext-steps", type=int, default=3,
+                    help="timed steps of the margin sweep and the large-n legs (the headline uses --steps)")
+    ap.add_argument("--details", default=os.path.join(ROOT, "bench_details.json"),
+                    help="where the full result tables are written")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-margins", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--batch-count", type=int, default=4096)
     ap.add_argument("--no-serve", action="store_true")
@@ -562,18 +775,24 @@ def main() -> None:
     import torch.distributed as dist
     from datetime import timedelta
     from hpcc_fpga_b200 import lpcuda as lp
+    from hpcc_fpga_b200.replicas import job_rate
 
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    cpu = CpuBaseline(args.cpu_n, args.cpu_reps) if (world == 1 and not args.no_cpu) else None
     n, bs = args.n, args.bs
     ctx = lp.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream)
+    pk = peaks()
+    ext_steps = max(1, min(args.steps, args.ext_steps))
+    ext_warm = max(1, min(args.warmup, 2))
 
     A, b64, b32 = lp.generate_baseline(n, 42, 1.0)
     with torch.cuda.stream(stream):
         dA0 = torch.from_numpy(A).to("cuda")
         dB0 = torch.from_numpy(b32).to("cuda")
+        dB64 = torch.from_numpy(b64).to("cuda")
         dA = torch.empty_like(dA0)
         dB = torch.empty_like(dB0)
     torch.cuda.synchronize()
@@ -610,17 +829,15 @@ def main() -> None:
     prof = ctx.read_profile(reset=True)
     launches = prof["kernel_launches"] - launches0
     ctx.set_profiling(False)
-    x = dB.cpu().numpy()
-    max_err = float(np.abs(x.astype(np.float64) - 1.0).max())
+    max_err = float((dB.double() - 1.0).abs().max())
     # HPL scaled residual of the plain FP32 solution (no refinement), in both
     # unit roundoffs, for the equal-residual comparison with the mixed forms.
     with torch.cuda.stream(stream):
-        dB64r = torch.from_numpy(b64).to("cuda")
         dXr = torch.empty(n, dtype=torch.float64, device="cuda")
-    r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64r.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
-    del dB64r, dXr
-    from hpcc_fpga_b200.replicas import job_rate
+    r32 = ctx.refine(dA0.data_ptr(), n, dA.data_ptr(), n, dB64.data_ptr(), dXr.data_ptr(), 1, 0)["hpl_resid"]
+    del dXr
     value, t_max = job_rate(args.steps * flops(n) / 1e9, elapsed, device="cuda")
+    f32_value = value / world
 
     # ---- roofline of the dominant kernel (the FP32 trailing update) ----
     inner = prof["inner"]
@@ -629,43 +846,70 @@ def main() -> None:
     peak_tf = NUM_SMS * FP32_LANES_PER_SM * 2 * sm_mhz * 1e6 / 1e12
     stage_share = {k: prof[k]["s"] / max(1e-12, sum(prof[s]["s"] for s in lp.STAGES)) for k in lp.STAGES}
     gesl = prof["gesl"]
-    pk = peaks()
+
+    full = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"FP32 LU without pivoting + solve, n={n}, block {bs}, 1 RHS, seeded diagonally "
+                               "dominant (seed 42, margin 1), b = A*ones",
+                   "n": n, "block": bs, "rhs": 1,
+                   "l2": f"inputs larger than L2 ({4 * n * n / 2**30:.0f} GiB matrix restored every step)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+        "max_abs_err_x": max_err,
+        "hpl_resid": {"eps_dbl_half": r32, "eps_flt_half": r32 * 2.0 ** -29,
+                      "note": "plain FP32 solution, HPL scaled residual (gmres.c:182-193) with eps = 2^-53 and "
+                              "with the FP32 unit roundoff 2^-24"},
+        "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)",
+                     "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": (achieved_tf / peak_tf) if achieved_tf else None,
+                     "peak_source": f"derived: {NUM_SMS} SMs x {FP32_LANES_PER_SM} FP32 lanes x 2 flop x median SM "
+                                    f"clock under load ({sm_mhz} MHz); MEASURED_PEAKS.json has no FP32 figure",
+                     "peak_short": f"derived FP32: {NUM_SMS}x{FP32_LANES_PER_SM}x2x{sm_mhz:.0f}MHz",
+                     "per_unit": "2*m*m*bs flop per trailing update of an m x m trailing matrix",
+                     "launches": inner["calls"],
+                     # DRAM bytes per trailing update: the n=8192 ncu capture of this kernel
+                     # (profiles/k_sgemm_update_n8192_b512.md) read+wrote 452.4 MB for 503.3 MB of
+                     # algorithmic bytes; scaled by the algorithmic bytes of this run's updates.
+                     "traffic": (inner["bytes"] / inner["calls"] * 452.4 / 503.3) if inner["calls"] else None,
+                     "traffic_unit": "bytes per trailing update (scaled from the n=8192 capture)"},
+        "stages": {k: {"s": prof[k]["s"], "share": stage_share[k], "calls": prof[k]["calls"]} for k in lp.STAGES
+                   if prof[k]["calls"]},
+        "gesl": {"s_per_step": gesl["s"] / max(1, args.steps),
+                 "GBps": gesl["bytes"] / gesl["s"] / 1e9 if gesl["s"] > 0 else None,
+                 "frac_hbm": (gesl["bytes"] / gesl["s"] / 1e9 / pk["hbm_gbs"]) if gesl["s"] > 0 else None},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "peaks": pk,
+    }
+    # the allocation-free substitution on the same factors
+    full["gesl_noalloc"] = run_gesl_noalloc(lp, torch, stream, dA, dB0, n, ext_steps)
 
     mbs = args.mixed_bs or mixed_block(n, bs)
-    mixed = {}
     if not args.no_mixed and mbs % 128 == 0:
+        full["mixed"] = {}
         for prec in ("bf16", "fp8"):
-            mixed[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, b64, n, mbs, prec, args.steps,
-                                    max(1, min(args.warmup, 2)), value / world, pk)
-            mixed[prec]["block"] = mbs
+            full["mixed"][prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, dB64, n, mbs, prec, args.steps,
+                                            ext_warm, f32_value, pk)
+        if not args.no_margins:
+            full["margins"] = run_margin_sweep(ctx, lp, torch, stream, dA0, dA, n, mbs, ("bf16", "fp8"), ext_steps,
+                                               ext_warm, f32_value, pk, skip_margin_one=full["mixed"])
 
-    f32emu = None
     if not args.no_f32emu and mbs % 128 == 0:
-        f32emu = run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, b64, n, mbs, args.steps,
-                            max(1, min(args.warmup, 2)), value / world, pk)
+        full["f32_bf16x6"] = run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, dB64, n, mbs, ext_steps, ext_warm,
+                                        f32_value, pk)
 
-    pivot = None
     if not args.no_pivot:
-        pivot = run_pivot(ctx, lp, torch, stream, n, args.steps, max(1, min(args.warmup, 2)), pk)
-        if pivot is not None and pivot["roofline"]["achieved"]:
-            pivot["roofline"]["peak"] = peak_tf
-            pivot["roofline"]["frac"] = pivot["roofline"]["achieved"] / peak_tf
+        full["pivot"] = run_pivot(ctx, lp, torch, stream, n, ext_steps, ext_warm, peak_tf)
 
-    fp64 = None
     if not args.no_fp64 and n % 256 == 0:
-        fp64 = run_fp64(ctx, lp, torch, stream, A, b64, n, args.steps, max(1, min(args.warmup, 2)),
-                        NUM_SMS * 64 * 2 * sm_mhz * 1e6 / 1e12)
+        full["fp64"] = run_fp64(ctx, lp, torch, stream, dA0, dB64, n, ext_steps, ext_warm,
+                                NUM_SMS * 64 * 2 * sm_mhz * 1e6 / 1e12)
 
-    batched = None
     if not args.no_batch:
-        batched = run_batched(ctx, lp, torch, stream, args.steps, max(1, min(args.warmup, 2)), args.batch_count)
-
-    serving = None
-    if not args.no_serve and world == 1:
-        serving = run_serving(lp, [float(r) for r in args.serve_rates.split(",")], args.serve_precisions.split(","))
+        full["batched"] = run_batched(ctx, lp, torch, stream, ext_steps, ext_warm, args.batch_count)
 
     # ---- end to end through the C ABI with pinned host buffers ----
-    e2e = None
     if not args.no_e2e:
         L = lp.lib()
         pa, pb = ctypes.c_void_p(), ctypes.c_void_p()
@@ -685,67 +929,63 @@ def main() -> None:
         walls = walls[1:]
         e2e_err = float(np.abs(hb.astype(np.float64) - 1.0).max())
         e2e_value, wt = job_rate(args.steps * flops(n) / 1e9, sum(walls), device="cuda")
-        e2e = {"value": e2e_value, "unit": UNIT,
-               "h2d_bytes_per_step": 4 * n * n + 4 * n, "d2h_bytes_per_step": 4 * n * n + 4 * n,
-               "ms_per_step": 1e3 * wt / args.steps, "max_abs_err_x": e2e_err,
-               "api": "lp_calculate (C ABI, pinned host A and b)"}
+        full["e2e"] = {"value": e2e_value, "unit": UNIT,
+                       "h2d_bytes_per_step": 4 * n * n + 4 * n, "d2h_bytes_per_step": 4 * n * n + 4 * n,
+                       "ms_per_step": 1e3 * wt / args.steps, "max_abs_err_x": e2e_err,
+                       "api": "lp_calculate (C ABI, pinned host A and b)"}
+        del hA, hb
         L.lp_host_free(pa)
         L.lp_host_free(pb)
+
+    # ---- the second, larger system: FP32 against the mixed forms and their margin sweep ----
+    del dA0, dA, dB0, dB, dB64, A
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    nl = args.large_n
+    if nl and not args.no_mixed:
+        lbs = args.mixed_bs or mixed_block(nl, bs)
+        Al, bl64, _ = lp.generate_baseline(nl, 42, 1.0)
+        with torch.cuda.stream(stream):
+            dA0 = torch.from_numpy(Al).to("cuda")
+            dB64 = torch.from_numpy(bl64).to("cuda")
+            dA = torch.empty_like(dA0)
+            dB0 = dB64.float()
+            dB = torch.empty_like(dB0)
+        torch.cuda.synchronize()
+        del Al
+        f = run_f32(ctx, lp, torch, stream, dA0, dA, dB0, dB, nl, bs, ext_steps, 1)
+        f["frac"] = f["inner_tflops"] / peak_tf if f["inner_tflops"] else None
+        large = {"n": nl, "f32": f}
+        for prec in ("bf16", "fp8"):
+            large[prec] = run_mixed(ctx, lp, torch, stream, dA0, dA, dB64, nl, lbs, prec, ext_steps, 1, f["value"],
+                                    pk, with_gmres=False)
+        full["large"] = large
+        if not args.no_margins:
+            full["margins"] = full.get("margins", []) + run_margin_sweep(
+                ctx, lp, torch, stream, dA0, dA, nl, lbs, ("bf16", "fp8"), ext_steps, 1, f["value"], pk,
+                skip_margin_one=large)
+        del dA0, dA, dB0, dB, dB64
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    if cpu is not None:
+        full["cpu_baseline"] = cpu.result()
+
+    if not args.no_serve and world == 1:
+        full["serving"] = run_serving(lp, [float(r) for r in args.serve_rates.split(",")],
+                                      args.serve_precisions.split(","))
 
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return
-    line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"plain FP32 LU without pivoting + forward/back substitution, n={n}, block {bs}, "
-                               "1 RHS, seed 42 mt19937 diagonally dominant (margin 1), b = A*ones",
-                   "n": n, "block": bs, "precision": "f32", "rhs": 1,
-                   "l2": f"inputs larger than L2 ({4 * n * n / 2**30:.1f} GiB matrix, restored every step)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-        "max_abs_err_x": max_err,
-        "hpl_resid": {"eps_dbl_half": r32, "eps_flt_half": r32 * 2.0 ** -29,
-                      "note": "plain FP32 solution, HPL scaled residual (gmres.c:182-193) with eps = 2^-53 and "
-                              "with the FP32 unit roundoff 2^-24"},
-        "roofline": {"bound": "fp32_simt", "kernel": "k_sgemm_update (inner stage)",
-                     "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
-                     "frac": (achieved_tf / peak_tf) if achieved_tf else None,
-                     "peak_source": f"derived: {NUM_SMS} SMs x {FP32_LANES_PER_SM} FP32 lanes x 2 flop x median SM "
-                                    f"clock under load ({sm_mhz} MHz); MEASURED_PEAKS.json has no FP32 figure",
-                     "per_unit": "2*m*m*bs flop per trailing update of an m x m trailing matrix",
-                     "launches": inner["calls"],
-                     # DRAM bytes per trailing update: the n=8192 ncu capture of this kernel
-                     # (profiles/k_sgemm_update_n8192_b512.md) read+wrote 452.4 MB for 503.3 MB of
-                     # algorithmic bytes; scaled by the algorithmic bytes of this run's updates.
-                     "traffic": (inner["bytes"] / inner["calls"] * 452.4 / 503.3) if inner["calls"] else None,
-                     "traffic_unit": "bytes per trailing update (scaled from the n=8192 capture)"},
-        "stages": {k: {"s": prof[k]["s"], "share": stage_share[k], "calls": prof[k]["calls"]} for k in lp.STAGES
-                   if prof[k]["calls"]},
-        "gesl": {"s_per_step": gesl["s"] / max(1, args.steps),
-                 "GBps": gesl["bytes"] / gesl["s"] / 1e9 if gesl["s"] > 0 else None,
-                 "frac_hbm": (gesl["bytes"] / gesl["s"] / 1e9 / pk["hbm_gbs"]) if gesl["s"] > 0 else None},
-        "gpu_launches": launches,
-        "clocks": clk,
-    }
-    if mixed:
-        line["mixed"] = mixed
-    if f32emu is not None:
-        line["f32_bf16x6"] = f32emu
-    if pivot is not None:
-        line["pivot"] = pivot
-    if fp64 is not None:
-        line["fp64"] = fp64
-    if batched is not None:
-        line["batched"] = batched
-    if serving is not None:
-        line["serving"] = serving
-    if e2e is not None:
-        line["e2e"] = e2e
-    if world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_n, args.cpu_reps)
-    print(json.dumps(line), flush=True)
+    full["details"] = os.path.relpath(args.details, ROOT) if args.details.startswith(ROOT) else args.details
+    try:
+        with open(args.details, "w") as fh:
+            json.dump(full, fh, indent=1, default=str)
+    except OSError as exc:
+        full["details"] = f"not written: {exc}"
+    print(dumps_line(compact_line(full)), flush=True)
     if world > 1:
         dist.destroy_process_group()
 

@@ -180,8 +180,13 @@ __device__ __forceinline__ void block_matvec(const float* M, const float* acc, f
     __syncthreads();
 }
 
-constexpr int kSpinLimit = 1 << 22;  // x ~100 ns per poll: well under a second
+constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;  // a bounded wait gives up after 250 ms
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 __device__ __forceinline__ int ld_acquire(const int* p) {
     int v;
     asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -191,21 +196,26 @@ __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Lane 0 of the calling warp polls flag f (bounded); the warp then proceeds
-// together.  false: the wait gave up or another CTA aborted (err set).
+// Lane 0 of the calling warp polls flag f (bounded by kWaitLimitNs); the warp
+// then proceeds together.  false: the wait gave up or another CTA aborted
+// (err set).
 __device__ __forceinline__ bool warp_wait_flag(const int* f, int* err) {
     int ok = 1;
     if ((threadIdx.x & 31) == 0) {
         ok = 0;
-        for (int it = 0; it < kSpinLimit; it++) {
+        const unsigned long long t0 = global_ns();
+        for (;;) {
             if (ld_acquire(f) != 0) {
                 ok = 1;
                 break;
             }
             if (*(volatile int*)err != 0) break;
+            if (global_ns() - t0 > kWaitLimitNs) {
+                atomicExch(err, 1);
+                break;
+            }
             __nanosleep(64);
         }
-        if (!ok) atomicExch(err, 1);
     }
     ok = __shfl_sync(0xffffffffu, ok, 0);
     __syncwarp();
@@ -222,7 +232,7 @@ __global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, 
                                                    int ldi, const float* __restrict__ wprev, float* __restrict__ w,
                                                    int ldw, float* __restrict__ out, int ldo, int nrhs,
                                                    int* __restrict__ flags, int* __restrict__ ticket,
-                                                   int* __restrict__ err) {
+                                                   int* __restrict__ err, const int* __restrict__ never) {
     extern __shared__ __align__(16) float smem[];
     float* op = smem;                 // 128 x 128 block operator
     float* red = op + BLK2;           // 8 x NR x 128 partial sums
@@ -276,7 +286,8 @@ __global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, 
                     v[r].w = (row < kbK && col + 3 < n) ? src[3] : 0.0f;
                 }
             }
-            if (!warp_wait_flag(&flags[K], err)) {
+            // never (tests only): the second tile waits on a word that nothing sets
+            if (!warp_wait_flag((never != nullptr && t == 1 && s == 0) ? never : &flags[K], err)) {
                 ok = false;
                 break;
             }
@@ -334,21 +345,21 @@ constexpr size_t sweep_smem() {
 
 template <int NR>
 int sweeps(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* w1, float* w2, const float* inv,
-           int* sync, int sms, cudaStream_t st) {
+           int* sync, int* err, bool stall, int sms, cudaStream_t st) {
     const int nblk = (n + SB - 1) / SB;
     int* flags_f = sync;
     int* flags_b = sync + nblk;
     int* tickets = sync + 2 * nblk;
-    int* err = tickets + 2;
-    LP_CUDA(cudaMemsetAsync(sync, 0, sizeof(int) * (2 * (size_t)nblk + 2), st));  // the error word persists
+    const int* never = stall ? tickets + 2 : nullptr;
+    LP_CUDA(cudaMemsetAsync(sync, 0, sizeof(int) * gesl_sync_ints(n), st));  // err is the caller's
     const int per_sm = NR >= 16 ? 1 : 2;
     const int grid = std::min(nblk, per_sm * sms);
     // forward: b -> y (w2)
     k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, b, ldb, w2, w2, n, nullptr, 0, nrhs,
-                                                              flags_f, tickets, err);
+                                                              flags_f, tickets, err, never);
     // backward: y (w2) -> s (w1), x -> b
     k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, w2, n, w1, w1, n, b, ldb, nrhs,
-                                                               flags_b, tickets + 1, err);
+                                                               flags_b, tickets + 1, err, nullptr);
     count_launch(2);
     LP_CUDA(cudaGetLastError());
     return LP_OK;
@@ -388,13 +399,17 @@ int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_
     return LP_OK;
 }
 
-// Sync words of the persistent sweeps: flags of both directions, two tickets, an error word.
+// Sync words of the persistent sweeps: flags of both directions, two tickets,
+// and one word that nothing sets (the target of the test stall).
 size_t gesl_sync_ints(int n) { return 2 * (size_t)((n + SB - 1) / SB) + 3; }
 
-// Forward + back substitution with precomputed block inverses; sync: gesl_sync_ints(n)
-// zero-initialised ints whose last one is the error word (non-zero after a wait gave up).
+// Forward + back substitution with precomputed block inverses; sync:
+// gesl_sync_ints(n) ints (cleared here); err: an error word the caller zeroes
+// and reads (set when a bounded wait gave up; that tile is written as NaN).
+// stall (tests only): the forward sweep's second tile waits on a word that
+// nothing sets, so its bounded wait runs out.
 int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
-                    int* sync, cudaStream_t st) {
+                    int* sync, int* err, bool stall, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return LP_OK;
     if (lda % 4 != 0 || !aligned16(a)) return fail(LP_E_INVALID, "gesl: factors need lda % 4 == 0, 16-byte aligned");
     int dev = 0, sms = 0;
@@ -406,11 +421,11 @@ int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs,
         float* w1 = work;
         float* w2 = work + (size_t)n * g;
         if (g == 1)
-            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
+            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
         else if (g <= 4)
-            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
+            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
         else
-            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, sms, st));
+            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
     }
     return LP_OK;
 }

@@ -451,15 +451,35 @@ int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, i
     const size_t wf = gesl_work_floats(n, nrhs), si = gesl_sync_ints(n);
     LP_CHECK(c->gw.ensure(sizeof(float) * wf + sizeof(int) * si));
     LP_CHECK(c->ginv.ensure(sizeof(float) * gesl_inv_floats(n)));
+    LP_CHECK(c->gerr.ensure(sizeof(int)));
     float* inv = static_cast<float*>(c->ginv.ptr);
     float* work = static_cast<float*>(c->gw.ptr);
     int* sync = reinterpret_cast<int*>(work + wf);
-    LP_CUDA(cudaMemsetAsync(sync + si - 1, 0, sizeof(int), st));  // error word of the sweeps
+    const bool stall = c->stall_site == LP_STALL_GESL;
+    c->stall_site = stall ? 0 : c->stall_site;
     const int e = prof_begin(c, st);
     LP_CHECK(launch_diag_inverses(dLU, lda, n, inv, st));
-    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, work, inv, sync, st));
+    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, work, inv, sync, static_cast<int*>(c->gerr.ptr), stall, st));
     const double nn = n;
     return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
+}
+
+int gesl_clear(lp_ctx* c, cudaStream_t st) {
+    LP_CHECK(c->gerr.ensure(sizeof(int)));
+    LP_CUDA(cudaMemsetAsync(c->gerr.ptr, 0, sizeof(int), st));
+    return LP_OK;
+}
+
+int gesl_status(lp_ctx* c, cudaStream_t st, const char* who) {
+    if (c->hstat == nullptr) LP_CUDA(cudaMallocHost(&c->hstat, sizeof(int)));
+    LP_CHECK(c->gerr.ensure(sizeof(int)));
+    *c->hstat = 0;
+    LP_CUDA(cudaMemcpyAsync(c->hstat, c->gerr.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    LP_CHECK(wait_stream(c, st));
+    if (*c->hstat != 0)
+        return fail(LP_E_TIMEOUT, std::string(who) + ": a bounded wait of the substitution sweeps expired "
+                                                     "(the affected solution entries are NaN)");
+    return LP_OK;
 }
 
 static float elapsed_s(cudaEvent_t a, cudaEvent_t b) {
@@ -643,6 +663,12 @@ int lp_ctx_read_timeline(lp_ctx* c, lp_stage_event* out, int max, int* count) {
     return LP_OK;
 }
 
+int lp_ctx_test_stall(lp_ctx* c, int site) {
+    if (c == nullptr || site < 0 || site > LP_STALL_GESL) return fail(LP_E_INVALID, "lp_ctx_test_stall: bad argument");
+    c->stall_site = site;
+    return LP_OK;
+}
+
 int lp_host_alloc(size_t bytes, void** out) {
     if (out == nullptr || bytes == 0) return fail(LP_E_INVALID, "lp_host_alloc: bad argument");
     *out = nullptr;
@@ -706,7 +732,9 @@ int lp_gesl_dev(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs
     if (lda % 4 != 0 || !aligned16(dLU))
         return fail(LP_E_INVALID, "lp_gesl_dev: factors must be 16-byte aligned with lda a multiple of 4");
     LP_CUDA(cudaSetDevice(c->device));
-    return gesl_f32(c, dLU, n, lda, dB, nrhs, ldb, c->stream);
+    LP_CHECK(gesl_clear(c, c->stream));
+    LP_CHECK(gesl_f32(c, dLU, n, lda, dB, nrhs, ldb, c->stream));
+    return gesl_status(c, c->stream, "lp_gesl_dev");
 }
 
 int lp_gefa_prec_dev(lp_ctx* c, int precision, float* dA, int n, int lda, int bs) {
@@ -827,10 +855,12 @@ int lp_calculate(lp_ctx* c, int n, int lda, int bs, int repetitions, float* A, f
         }
         if (status != LP_OK) break;
         LP_CUDA(cudaEventRecord(c->ev[1], st));
-        status = gesl_f32(c, dA, n, lda, dB, 1, n, st);
+        status = gesl_clear(c, st);
+        if (status == LP_OK) status = gesl_f32(c, dA, n, lda, dB, 1, n, st);
         if (status != LP_OK) break;
         LP_CUDA(cudaEventRecord(c->ev[2], st));
-        LP_CUDA(cudaStreamSynchronize(st));
+        status = gesl_status(c, st, "lp_calculate");
+        if (status != LP_OK) break;
         gefa_times[rep] = elapsed_s(c->ev[0], c->ev[1]);
         gesl_times[rep] = elapsed_s(c->ev[1], c->ev[2]);
     }

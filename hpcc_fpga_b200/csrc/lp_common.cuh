@@ -111,7 +111,7 @@ size_t gesl_work_floats(int n, int nrhs);
 // The same with precomputed inverses of the 128 x 128 diagonal blocks (k_gesl_inv.cu).
 int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_t s);
 int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
-                    int* sync, cudaStream_t s);
+                    int* sync, int* err, bool stall, cudaStream_t st);
 size_t gesl_sync_ints(int n);
 size_t gesl_inv_floats(int n);
 int gesl_inv_init_attrs();

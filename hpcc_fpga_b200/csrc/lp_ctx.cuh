@@ -64,6 +64,11 @@ constexpr int kBatchSolveOnly = 1 << 8;
 int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, const double* b64, double* x, int nrhs,
                 int max_iters, int* iters, double* resid, cudaStream_t st);
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st);
+// The sweeps of gesl_f32 accumulate their error word in the context: gesl_clear
+// zeroes it (stream-ordered), gesl_status copies it back, waits for st and
+// returns LP_E_TIMEOUT (naming who) if a bounded wait gave up since the clear.
+int gesl_clear(lp_ctx* c, cudaStream_t st);
+int gesl_status(lp_ctx* c, cudaStream_t st, const char* who);
 // FP64 form (lp_fp64.cu): factorization and substitution in double.
 int gefa_f64(lp_ctx* c, double* a, int n, int lda, int bs, cudaStream_t st);
 int gesl_f64(lp_ctx* c, const double* a, int n, int lda, double* b, int nrhs, int ldb, cudaStream_t st);
@@ -127,6 +132,9 @@ struct lp_ctx {
     lp::Workspace tq;    // mixed panel: split-BF16 operands of the top and left products
     lp::Workspace gw;    // substitution work vectors
     lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
+    lp::Workspace gerr;  // error word of the substitution sweeps (non-zero: a bounded wait gave up)
+    int* hstat = nullptr;                     // pinned host copy of an error word
+    int stall_site = 0;                       // lp_ctx_test_stall: the next wait of this site never completes
     lp::Workspace dA, dA0, dB;                // host-entry-point matrix, original copy, FP32 rhs
     int fac_n = 0, fac_lda = 0, fac_prec = -1;  // factors resident in dA (lp_factor); fac_n 0: none
     lp::Workspace dB64, dX, dR, dCol;         // FP64 rhs, solution, residual, column sums
@@ -155,7 +163,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &ginv, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &ginv, &gerr, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
                                 &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
@@ -170,5 +178,7 @@ struct lp_ctx {
         if (hgm != nullptr) cudaFreeHost(hgm);
         hgm = nullptr;
         hgm_cap = 0;
+        if (hstat != nullptr) cudaFreeHost(hstat);
+        hstat = nullptr;
     }
 };

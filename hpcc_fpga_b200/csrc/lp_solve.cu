@@ -56,6 +56,7 @@ int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, con
     LP_CHECK(launch_rhs_absmax(dCol, n, n, 1, dn, st));
     LP_CHECK(launch_rhs_absmax(b64, n, n, nrhs, dn + 2, st));
     LP_CHECK(launch_f64_to_f32(dB, b64, nv, st));
+    LP_CHECK(gesl_clear(c, st));
     LP_CHECK(gesl_f32(c, lu, n, lda, dB, nrhs, n, st));
     LP_CHECK(launch_f32_to_f64(x, dB, nv, st));
     LP_CUDA(cudaEventRecord(c->ev[4], st));  // end of the first solve
@@ -68,7 +69,7 @@ int refine_core(lp_ctx* c, const float* a0, int lda, const float* lu, int n, con
         LP_CHECK(launch_rhs_absmax(dR, n, n, nrhs, rn, st));
         LP_CHECK(launch_rhs_absmax(x, n, n, nrhs, xn, st));
         LP_CUDA(cudaMemcpyAsync(c->hnorm, dn, sizeof(unsigned long long) * slots, cudaMemcpyDeviceToHost, st));
-        LP_CHECK(wait_stream(c, st));
+        LP_CHECK(gesl_status(c, st, "refinement"));  // waits for st
         const unsigned long long* h = c->hnorm;
         const double normA = from_bits(h[0]);
         resid = 0.0;

@@ -26,6 +26,7 @@ LP_E_BUDGET = -7
 LP_E_NODEVICE = -8
 
 LP_F32, LP_BF16_IR, LP_FP8_IR, LP_F32_BF16X6 = 0, 1, 2, 3
+LP_STALL_NONE, LP_STALL_GESL = 0, 1
 PRECISIONS = {"f32": LP_F32, "bf16": LP_BF16_IR, "fp8": LP_FP8_IR, "f32_bf16x6": LP_F32_BF16X6}
 
 _F32P = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -156,6 +157,7 @@ def lib() -> ctypes.CDLL:
     L.lp_ctx_set_profiling.argtypes = [_VP, _I]
     L.lp_ctx_read_profile.argtypes = [_VP, ctypes.POINTER(LpProfile), _I]
     L.lp_ctx_read_timeline.argtypes = [_VP, ctypes.POINTER(LpStageEvent), _I, ctypes.POINTER(_I)]
+    L.lp_ctx_test_stall.argtypes = [_VP, _I]
     L.lp_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(_VP)]
     L.lp_host_free.argtypes = [_VP]
     L.lp_lu_block_dev.argtypes = [_VP, _VP, _I, _I]
@@ -298,6 +300,10 @@ class Context:
         k = _I(0)
         check(lib().lp_ctx_read_timeline(self._h, out, max_events, ctypes.byref(k)), "lp_ctx_read_timeline")
         return [(STAGES[out[i].stage], out[i].stream, out[i].t0_s, out[i].t1_s) for i in range(k.value)]
+
+    def test_stall(self, site: int) -> None:
+        """Arm a bounded wait that runs out (failure-path tests): see lp_ctx_test_stall."""
+        check(lib().lp_ctx_test_stall(self._h, site), "lp_ctx_test_stall")
 
     def read_profile(self, reset: bool = True) -> dict:
         p = LpProfile()

@@ -130,6 +130,19 @@ typedef struct {
 /* Copies up to max entries of the stage timeline into out (*count of them). */
 int lp_ctx_read_timeline(lp_ctx* ctx, lp_stage_event* out, int max, int* count);
 
+/* ---- failure-path test hook (no counterpart in the reference) ------------
+ * Every wait inside this library's kernels is bounded: a kernel that gives up
+ * records an error word, finishes without touching memory it does not own,
+ * and the entry point returns LP_E_TIMEOUT with the context still usable.
+ * lp_ctx_test_stall arms that path for tests: the next substitution sweep on
+ * this context (LP_STALL_GESL) makes one tile wait on a word that nothing
+ * sets, so its bounded wait (250 ms) runs out; the call then returns
+ * LP_E_TIMEOUT and the affected solution entries are NaN.  The stall is used
+ * once; site 0 disarms it. */
+#define LP_STALL_NONE 0
+#define LP_STALL_GESL 1
+int lp_ctx_test_stall(lp_ctx* ctx, int site);
+
 /* ---- block stages (device pointers) -------------------------------------
  * The four kernels of LINPACK/src/device/hpl_torus_PCIE.cl, as whole-panel
  * launches.  bs is the block size (power of two, 16..512). */
@@ -194,7 +207,9 @@ int lp_gmres_dev(lp_ctx* ctx, const float* dA0, int lda, const float* dLU, int n
                  int restart, int max_it, double tol, lp_timing* t);
 /* Forward + back substitution with the encoded factors for nrhs right-hand
  * sides stored as rows of dB (dB[r*ldb + i]); the solutions overwrite dB.
- * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229). */
+ * Device version of gesl_ref_nopvt (linpack_data.cpp:199-229).  Returns once
+ * the solve has finished on the device: it reads back the sweeps' error word
+ * and returns LP_E_TIMEOUT if one of their bounded waits expired. */
 int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb);
 
 /* The same substitution for callers that cannot allocate device memory: no
@@ -206,11 +221,18 @@ int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nr
  * live in one fixed device array of 2^20 floats (4 MiB) that every GPU which
  * loads the library holds until the process exits, so it accepts only
  * 2 * n * min(nrhs, 16) <= 1048576 and returns LP_E_INVALID beyond that.
+ * It runs the blocked substitution kernels k_gesl_fwd / k_gesl_bwd (one
+ * launch per 128-row block and direction, no inverses of the diagonal blocks)
+ * rather than lp_gesl_dev's persistent sweeps, whose inverses would need
+ * more scratch; the results agree to FP32 rounding.
  * The first call on a device (the current device) looks up the array's
  * address and sets kernel attributes for that device; make that first call
- * before any stream capture.  All calls share the array and each call fully
- * rewrites what it reads, but calls whose work overlaps on the GPU (other
- * streams, other threads, same device) race on it: serialize them.
+ * before any stream capture.  The address is looked up in, and cached for, the
+ * device's primary context (the one the CUDA runtime uses): a caller that
+ * drives the device through another driver-API context must not use this
+ * entry point.  All calls share the array and each call fully rewrites what
+ * it reads, but calls whose work overlaps on the GPU (other streams, other
+ * threads, same device) race on it: serialize them.
  * stream: a cudaStream_t, or NULL for the default stream.  dLU, dB as for
  * lp_gesl_dev; the solutions overwrite dB. */
 int lp_gesl_dev_noalloc(const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, void* stream);

@@ -36,13 +36,27 @@ _ref32 = None
 _ref64 = None
 
 
-def build(reference_root: str | None = None) -> None:
-    """Build the restatement and, when the reference sources exist, the
-    reference libraries (``make -C oracle``)."""
-    args = ["make", "-s", "-C", _HERE, "orc"]
-    subprocess.run(args, check=True)
-    root = reference_root or "/root/reference"
-    if os.path.isdir(os.path.join(root, "LINPACK", "src", "host")):
+REFERENCE_ENV = "HPCC_FPGA_REFERENCE"
+
+
+def reference_root(explicit: str | None = None) -> str | None:
+    """Where the reference checkout is read from: the explicit argument, else
+    $HPCC_FPGA_REFERENCE, else a checkout named ``reference`` beside this
+    repository; None when none of them holds LINPACK's host sources."""
+    repo = os.path.dirname(_HERE)
+    for cand in (explicit, os.environ.get(REFERENCE_ENV), os.path.join(os.path.dirname(repo), "reference")):
+        if cand and os.path.isdir(os.path.join(cand, "LINPACK", "src", "host")):
+            return cand
+    return None
+
+
+def build(reference_root_dir: str | None = None) -> None:
+    """Build the restatement and, when the reference sources are found
+    (reference_root), the reference libraries (``make -C oracle``).  Without
+    them the prebuilt files already in ``_ref/`` are used as they are."""
+    subprocess.run(["make", "-s", "-C", _HERE, "orc"], check=True)
+    root = reference_root(reference_root_dir)
+    if root is not None:
         subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF_ROOT={root}"], check=True)
 
 

@@ -157,3 +157,51 @@ def test_mixed_rejects_small_block(ctx, lp):
     with pytest.raises(lp.LpError) as e:
         ctx.solve_host(A, np.ones(256), 64, "bf16")
     assert e.value.status == lp.LP_E_INVALID
+
+
+@pytest.fixture(scope="module")
+def seeded_systems(dev, lp):
+    """Device copies of seeded workload matrices, drawn once per (n, seed)."""
+    cache = {}
+
+    def get(n, seed):
+        if (n, seed) not in cache:
+            A, _, _ = lp.generate_baseline(n, seed, 1.0)
+            cache[(n, seed)] = dev.put(A)
+        return cache[(n, seed)]
+
+    yield get
+    cache.clear()
+
+
+@pytest.mark.parametrize("seed", [42, 7])
+@pytest.mark.parametrize("bs", [1024, 2048])
+def test_mixed_large_blocks_margin_sweep(ctx, dev, seeded_systems, seed, bs):
+    """The schedules the benchmark runs at n = 32768 (block 1024) and
+    n = 65536 (block 2048, plain BF16 panel products), here at n = 16384 over
+    the diagonal-dominance margins {1, 0.1 sqrt(n), n} and two seeds: BF16 and
+    FP8 factors refine in FP64 to the HPL threshold (gmres.c:182-193) in at
+    most five refinements, and the FP64-oracle error (the exact solution is
+    all ones) stays below 1e-8: two orders under an FP32-accurate solution
+    (~1e-6 here), so a refinement that stalls at the factors' precision fails,
+    while the largest error measured at n = 65536 (2.6e-10) passes."""
+    from hpcc_fpga_b200.workload import set_margin
+
+    torch = dev.torch
+    n = 16384
+    dA0 = seeded_systems(n, seed)
+    for margin in (1.0, 0.1 * n ** 0.5, float(n)):
+        dB64 = set_margin(torch, dA0, n, margin)
+        for prec in ("bf16", "fp8"):
+            dLU = dA0.clone()
+            ctx.gefa_prec(prec, dLU.data_ptr(), n, n, bs)
+            dX = dev.empty((n,), np.float64)
+            t = ctx.refine(dA0.data_ptr(), n, dLU.data_ptr(), n, dB64.data_ptr(), dX.data_ptr(), 1, 50)
+            err = float((dX - 1.0).abs().max())
+            case = f"seed {seed} block {bs} margin {margin:g} {prec}: hpl {t['hpl_resid']:.3g} " \
+                   f"iters {t['ir_iters']} err {err:.3g}"
+            assert t["hpl_resid"] <= 16.0, case
+            assert 1 <= t["ir_iters"] <= 5, case
+            assert err < 1e-8, case
+            del dLU, dX
+

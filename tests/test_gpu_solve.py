@@ -197,3 +197,36 @@ def test_bad_sizes_rejected(ctx, lp):
     with pytest.raises(lp.LpError) as e:
         ctx.calculate(A, np.zeros(100, np.float32), 64)
     assert e.value.status == lp.LP_E_INVALID
+
+
+@pytest.mark.parametrize("api", ["gesl_dev", "calculate", "solve_host"])
+def test_substitution_wait_that_runs_out_reports_timeout(ctx, dev, lp, api):
+    """A bounded wait of the substitution sweeps that runs out (armed by
+    lp_ctx_test_stall: one tile waits on a word that nothing sets) must come
+    back as LP_E_TIMEOUT through every entry point that runs the sweeps, with
+    no GPU fault, and leave the context usable: the next identical call
+    succeeds and validates."""
+    n, bs = 1024, 128
+    A, b, _, normb = oracle.gen_reference(n)
+
+    def run():
+        if api == "gesl_dev":
+            LU = oracle.gefa_nopvt(A)
+            dLU, dB = dev.put(LU), dev.put(b)
+            ctx.gesl(dLU.data_ptr(), n, n, dB.data_ptr(), 1, n)
+            return dev.get(dB)
+        if api == "calculate":
+            Ac, bc = A.copy(), b.copy()
+            ctx.calculate(Ac, bc, bs, repetitions=1)
+            return bc
+        x, _ = ctx.solve_host(A.copy(), b.astype(np.float64), bs, "bf16", max_iters=10)
+        return x
+
+    ctx.test_stall(lp.LP_STALL_GESL)
+    with pytest.raises(lp.LpError) as e:
+        run()
+    assert e.value.status == lp.LP_E_TIMEOUT
+    assert "bounded wait" in str(e.value)
+    x = run()  # the stall was used once; the context still works
+    residn, _ = oracle.residn(np.asarray(x, np.float32), normb)
+    assert np.all(np.isfinite(x)) and residn < 1.0

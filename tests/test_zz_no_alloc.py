@@ -4,7 +4,14 @@ or they sit in a serving loop where an allocation may stall the device).  Its
 work vectors live in one fixed 4 MiB device array instead of a context
 workspace.  Checked through the C ABI against lp_gesl_dev, the allocating
 entry point, on two calls in a row (the second call reuses the array with the
-first call's contents still in it).  This file is collected last on purpose."""
+first call's contents still in it).  This file is collected last on purpose.
+
+The two entry points run different kernels: lp_gesl_dev inverts the 128 x 128
+diagonal blocks (k_inv_top / k_inv_left) and solves in two persistent sweeps
+(k_gesl_sweep); lp_gesl_dev_noalloc runs one k_gesl_fwd / k_gesl_bwd launch
+per 128-row block and direction.  Both sum in a different order from the
+oracle, so each is held to the FP64 solution of the same factors with a
+bound scaled by the FP32 oracle's own error, and to each other."""
 import numpy as np
 import pytest
 
@@ -14,11 +21,12 @@ pytestmark = pytest.mark.gpu
 FLT_EPS = float(np.finfo(np.float32).eps)
 
 
-def _solve_noalloc(lp, dev, dLU, n, B):
-    dB = dev.put(B)
+def _solve_noalloc(lp, torch, dLU, n, B):
+    dB = torch.from_numpy(np.ascontiguousarray(B)).cuda()
+    torch.cuda.synchronize()
     st = lp.lib().lp_gesl_dev_noalloc(dLU.data_ptr(), n, n, dB.data_ptr(), B.shape[0], n, None)
     lp.check(st, "lp_gesl_dev_noalloc")
-    dev.torch.cuda.synchronize()
+    torch.cuda.synchronize()
     return dB.cpu().numpy()
 
 
@@ -28,8 +36,10 @@ def _solve_alloc(ctx, dev, dLU, n, B):
     return dev.get(dB)
 
 
-@pytest.mark.parametrize("n,nrhs", [(1024, 1), (768, 5)])
+@pytest.mark.parametrize("n,nrhs", [(1024, 1), (768, 5), (512, 20)])
 def test_noalloc_matches_allocating_entry_point_twice(ctx, dev, lp, n, nrhs):
+    """nrhs = 20 runs two chunks (16 + 4 right-hand sides) through the shared
+    array within one call."""
     A, _, _, _ = oracle.gen_reference(n)
     LU = oracle.gefa_nopvt(A)
     dLU = dev.put(LU)
@@ -38,15 +48,41 @@ def test_noalloc_matches_allocating_entry_point_twice(ctx, dev, lp, n, nrhs):
     for call in range(2):
         B = rng.uniform(-1, 1, (nrhs, n)).astype(np.float32)
         want = _solve_alloc(ctx, dev, dLU, n, B)
-        got = _solve_noalloc(lp, dev, dLU, n, B)
-        # Same kernels as lp_gesl_dev, so the tolerance of the substitution
-        # tests (test_gpu_solve.py::test_gesl_multi_rhs) holds a fortiori.
+        got = _solve_noalloc(lp, dev.torch, dLU, n, B)
         for r in range(nrhs):
             x64 = oracle.gesl_nopvt(LU64, B[r].astype(np.float64))
             x32 = oracle.gesl_nopvt(LU, B[r])
             tol = 8 * np.abs(x32 - x64).max() + 64 * FLT_EPS * np.abs(x64).max()
             assert np.abs(got[r] - x64).max() <= tol, f"call {call}, rhs {r}"
+            assert np.abs(want[r] - x64).max() <= tol, f"call {call}, rhs {r} (lp_gesl_dev)"
         assert np.allclose(got, want, rtol=0, atol=64 * FLT_EPS * np.abs(want).max()), f"call {call}"
+
+
+def test_noalloc_at_the_scratch_limit(ctx, dev, lp):
+    """2 * n * min(nrhs, 16) == 2^20 exactly (n = 32768, 16 right-hand sides)
+    is accepted.  The factors come from lp_gefa_dev on a seeded diagonally
+    dominant matrix made on the device; the FP64 substitution of the same
+    factors (lp_gesl_f64_dev on the factors widened exactly) is the reference
+    solution for both entry points."""
+    torch = dev.torch
+    n, nrhs = 32768, 16
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5)
+    dA = torch.rand((n, n), generator=g, device="cuda", dtype=torch.float32) - 0.5
+    dA.diagonal().copy_(dA.abs().sum(1) + 1.0)
+    ctx.gefa(dA.data_ptr(), n, n, 512)
+    ctx.sync()
+    B = np.random.default_rng(11).uniform(-1, 1, (nrhs, n)).astype(np.float32)
+    dLU64 = dA.double()
+    dX64 = torch.from_numpy(B.astype(np.float64)).cuda()
+    ctx.gesl_f64(dLU64.data_ptr(), n, n, dX64.data_ptr(), nrhs, n)
+    x64 = dev.get(dX64)
+    del dLU64
+    for call in range(2):
+        want = _solve_alloc(ctx, dev, dA, n, B)
+        got = _solve_noalloc(lp, torch, dA, n, B)
+        err_alloc = np.abs(want - x64).max()
+        assert np.abs(got - x64).max() <= 8 * err_alloc + 64 * FLT_EPS * np.abs(x64).max(), f"call {call}"
 
 
 def test_noalloc_rejects_sizes_beyond_the_fixed_scratch(lp, dev):
@@ -57,3 +93,6 @@ def test_noalloc_rejects_sizes_beyond_the_fixed_scratch(lp, dev):
     st = lp.lib().lp_gesl_dev_noalloc(dLU.data_ptr(), n, n, dB.data_ptr(), 16, n, None)
     assert st == lp.LP_E_INVALID
     assert "fixed scratch" in lp.last_error()
+    # one row more than the limit allows, with 16 right-hand sides
+    st = lp.lib().lp_gesl_dev_noalloc(dLU.data_ptr(), 32769, 32772, dB.data_ptr(), 16, 32772, None)
+    assert st == lp.LP_E_INVALID
