@@ -1,31 +1,43 @@
-// gesl with inverted diagonal blocks — the substitution of the factorization
-// paths (the reference's gesl_ref_nopvt, LINPACK/src/host/linpack_data.cpp:199-229).
+// gesl with inverted diagonal blocks — the substitution of every path that
+// solves with FP32 factors (the reference's gesl_ref_nopvt,
+// LINPACK/src/host/linpack_data.cpp:199-229).
 //
-// For every 128 x 128 diagonal block D of the encoded factors two dense
-// operators are formed once per solve, all blocks in one launch:
-//   Y = (I - U)^-1             by the left recurrence on an identity (U: D's
-//                              strict upper storage triangle, the negated
-//                              multipliers);
-//   X = (diag(D_kk)^-1 - L)^-1 by the top recurrence on an identity (D_kk =
-//                              -1/d as stored; L: D's strict lower storage
-//                              triangle, the U factor of M).
-// Within a block the forward sweep is then y = Y^T acc and the backward sweep
-// s = X^T acc, x = -s: a 128 x 128 matrix-vector product over all 256 threads
-// instead of a 128-step sequential chain.
+// Storage terms (S[r][c] = a[r*lda + c]), blocked by SB = 128 unknowns:
+//   forward  acc_j = b_j + sum_{K<j} y_K^T S[K][j],  y_j = Y_j^T acc_j
+//   backward acc_j = y_j + sum_{K>j} s_K^T S[K][j],  s_j = X_j^T acc_j,  x_j = -s_j
+// with, for the diagonal block D of tile j,
+//   Y = (I - U)^-1             U: D's strict upper storage triangle (the
+//                              negated multipliers), by the left recurrence
+//                              applied to an identity;
+//   X = (diag(D_kk)^-1 - L)^-1 L: D's strict lower storage triangle (the U
+//                              factor of M), D_kk = -1/d as stored, by the top
+//                              recurrence applied to an identity.
+// Within a tile the sequential 128-step chain becomes one 128 x 128
+// matrix-vector product over all 256 threads.
 //
-// Each sweep is ONE persistent launch over 128-unknown tiles.  A CTA takes
-// tiles in ticket order (atomic counter: forward 0, 1, 2, ...; backward from
-// the last tile down) and accumulates, for its tile j, the contributions of
-// every earlier tile K: acc_j += y_K^T * S[rows of K][columns of j], reading
-// each factor element once.  It loads the factor rows of tile K before
-// waiting for K's "solved" flag, so the wait overlaps the memory traffic, and
-// keeps per-thread partial sums until all K are in; then it reduces them,
-// forms y_j with the block operator (prefetched into shared memory when the
-// tile started), publishes y_j and raises flag j.  A CTA only waits on tiles
-// taken before its own by running CTAs, so progress is guaranteed; every wait
-// is bounded nonetheless, and a CTA that gives up records the error, writes
-// NaN for its tile (the result then fails every residual check) and still
-// raises its flag so no other CTA waits on it.
+// Each sweep is ONE persistent launch, one CTA per SM.  A CTA takes tiles in
+// ticket order (forward 0, 1, 2, ...; backward from the last tile down) and,
+// for its tile j:
+//   1. starts streaming the factor blocks S[K][j] of every source tile K
+//      (forward K < j, backward K > j) through a 5-stage cp.async ring of
+//      32-row stages, so a whole source tile plus one stage is in flight;
+//   2. meanwhile inverts its own diagonal block into shared memory (Y or X:
+//      no separate launch, no global workspace for the operators);
+//   3. for each source tile waits for its published values (one poll loop
+//      over the tile's (value, tag) pairs), then adds its contributions;
+//   4. forms acc_j, multiplies by the operator, publishes its own values.
+// Published values are 64-bit pairs (tag << 32 | float bits), written with
+// relaxed stores and read with relaxed loads: a pair is valid on its own, so a
+// consumer needs one L2 round trip (no flag, then data).  The forward sweep
+// tags with 1, the backward sweep with 2 into the same array (it is cleared
+// before the forward sweep), and the backward sweep reads its input y_j
+// there.  A CTA only waits on tiles whose tickets were taken before its own
+// by running CTAs, so progress is guaranteed even when not every CTA is
+// resident; every wait is bounded nonetheless (250 ms by %globaltimer), and a
+// CTA that gives up records the error, writes NaN for its tile and still
+// publishes it, so no other CTA waits on it.  The summation order is fixed
+// (sources in order, rows in order, a fixed two-way reduction), so results
+// are deterministic.
 #include <algorithm>
 
 #include "gesl_common.cuh"
@@ -35,28 +47,33 @@ namespace {
 
 using namespace gesl;
 
-constexpr int ICH = 32;       // chunk of the inverse recurrences
-constexpr int IST = 64;       // strip width of the inverse kernels
-constexpr int BLK2 = SB * SB; // floats per operator
-constexpr size_t kInvTopSmem = sizeof(float) * (SB * IST + SB * ICH);
-constexpr size_t kInvLeftSmem = sizeof(float) * (IST * (SB + 1) + ICH * SB);
+constexpr int ICH = 32;        // chunk of the inverse recurrences
+constexpr int IST = 64;        // strip width of the inverse recurrences
+constexpr int BLK2 = SB * SB;  // floats per operator
+constexpr int RS = 32;         // factor rows per ring stage
+constexpr int SPT = SB / RS;   // stages per source tile
+constexpr int STAGES = SPT + 1;
+constexpr int STAGE_FLOATS = RS * SB;
+constexpr int kInvTopScratch = SB * IST + SB * ICH;
+constexpr int kInvLeftScratch = IST * (SB + 1) + ICH * SB;
+constexpr int kInvScratch = kInvTopScratch > kInvLeftScratch ? kInvTopScratch : kInvLeftScratch;
+constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;  // a bounded wait gives up after 250 ms
+constexpr unsigned kTagFwd = 1, kTagBwd = 2, kTagNever = 0x7fff0000u;
 
-// X of diagonal block blockIdx.y, columns [64*blockIdx.x, +64).
-__global__ void __launch_bounds__(256) k_inv_top(const float* __restrict__ a, int lda, int n, float* __restrict__ inv) {
-    extern __shared__ float ism[];
-    float* strip = ism;            // SB x IST
-    float* dch = ism + SB * IST;   // SB x ICH
+// Columns [c0, c0 + IST) of X for the diagonal block d (kb valid rows and
+// columns; the rest of the 128 x 128 block is the identity) into op (row
+// stride SB).  All 256 threads; scr: kInvTopScratch floats.
+__device__ void inv_top_strip(const float* __restrict__ d, int lda, int kb, int c0, float* scr, float* op) {
+    float* strip = scr;            // SB x IST
+    float* dch = scr + SB * IST;   // SB x ICH
     const int tid = threadIdx.x;
-    const int b = blockIdx.y, k0 = b * SB, kb = min(SB, n - k0);
-    const int c0 = blockIdx.x * IST;
-    const float* d = a + (size_t)k0 * lda + k0;
-    for (int idx = tid; idx < SB * IST; idx += 256) {
+    for (int idx = tid; idx < SB * IST; idx += GT) {
         const int r = idx / IST, c = idx - r * IST;
         strip[idx] = (r == c0 + c) ? 1.0f : 0.0f;
     }
     for (int r0 = 0; r0 < SB; r0 += ICH) {
         const int nr = SB - r0;
-        for (int idx = tid; idx < nr * ICH; idx += 256) {
+        for (int idx = tid; idx < nr * ICH; idx += GT) {
             const int rr = idx / ICH, kk = idx - rr * ICH;
             const int r = r0 + rr, k = r0 + kk;
             dch[idx] = (r < kb && k < kb) ? d[(size_t)r * lda + k] : (r == k ? 1.0f : 0.0f);
@@ -82,7 +99,7 @@ __global__ void __launch_bounds__(256) k_inv_top(const float* __restrict__ a, in
             float x[ICH];
 #pragma unroll
             for (int k = 0; k < ICH; k++) x[k] = strip[(r0 + k) * IST + c];
-            for (int r = r0 + ICH + g; r < SB; r += 256 / IST) {
+            for (int r = r0 + ICH + g; r < SB; r += GT / IST) {
                 float acc = strip[r * IST + c];
                 const float* drow = dch + (r - r0) * ICH;
 #pragma unroll
@@ -92,30 +109,27 @@ __global__ void __launch_bounds__(256) k_inv_top(const float* __restrict__ a, in
         }
         __syncthreads();
     }
-    float* out = inv + (size_t)b * 2 * BLK2;
-    for (int idx = tid; idx < SB * IST; idx += 256) {
+    for (int idx = tid; idx < SB * IST; idx += GT) {
         const int r = idx / IST, c = idx - r * IST;
-        out[r * SB + c0 + c] = strip[idx];
+        op[r * SB + c0 + c] = strip[idx];
     }
+    __syncthreads();
 }
 
-// Y of diagonal block blockIdx.y, rows [64*blockIdx.x, +64).
-__global__ void __launch_bounds__(256) k_inv_left(const float* __restrict__ a, int lda, int n, float* __restrict__ inv) {
+// Rows [r0s, r0s + IST) of Y for the diagonal block d into op (row stride
+// SB).  All 256 threads; scr: kInvLeftScratch floats.
+__device__ void inv_left_strip(const float* __restrict__ d, int lda, int kb, int r0s, float* scr, float* op) {
     constexpr int SL = SB + 1;
-    extern __shared__ float ism[];
-    float* strip = ism;            // IST x (SB + 1)
-    float* dch = ism + IST * SL;   // ICH x SB
+    float* strip = scr;            // IST x (SB + 1)
+    float* dch = scr + IST * SL;   // ICH x SB
     const int tid = threadIdx.x;
-    const int b = blockIdx.y, k0 = b * SB, kb = min(SB, n - k0);
-    const int r0s = blockIdx.x * IST;
-    const float* d = a + (size_t)k0 * lda + k0;
-    for (int idx = tid; idx < IST * SB; idx += 256) {
+    for (int idx = tid; idx < IST * SB; idx += GT) {
         const int rr = idx / SB, c = idx - rr * SB;
         strip[rr * SL + c] = (r0s + rr == c) ? 1.0f : 0.0f;
     }
     for (int c0 = 0; c0 < SB; c0 += ICH) {
         const int nc = SB - c0;
-        for (int idx = tid; idx < ICH * nc; idx += 256) {
+        for (int idx = tid; idx < ICH * nc; idx += GT) {
             const int kk = idx / nc, cc = idx - kk * nc;
             const int k = c0 + kk, c = c0 + cc;
             dch[idx] = (k < kb && c < kb) ? d[(size_t)k * lda + c] : 0.0f;
@@ -134,7 +148,7 @@ __global__ void __launch_bounds__(256) k_inv_left(const float* __restrict__ a, i
             for (int k = 0; k < ICH; k++) row[k] = x[k];
         }
         __syncthreads();
-        for (int ci = ICH + tid; ci < nc; ci += 256) {
+        for (int ci = ICH + tid; ci < nc; ci += GT) {
             float dv[ICH];
 #pragma unroll
             for (int k = 0; k < ICH; k++) dv[k] = dch[k * nc + ci];
@@ -148,11 +162,11 @@ __global__ void __launch_bounds__(256) k_inv_left(const float* __restrict__ a, i
         }
         __syncthreads();
     }
-    float* out = inv + (size_t)b * 2 * BLK2 + BLK2;
-    for (int idx = tid; idx < IST * SB; idx += 256) {
+    for (int idx = tid; idx < IST * SB; idx += GT) {
         const int rr = idx / SB, c = idx - rr * SB;
-        out[(r0s + rr) * SB + c] = strip[rr * SL + c];
+        op[(r0s + rr) * SB + c] = strip[rr * SL + c];
     }
+    __syncthreads();
 }
 
 // coef[r][i] = sum_k M[k][i] * acc[r][k] for a 128 x 128 operator M (shared
@@ -180,68 +194,85 @@ __device__ __forceinline__ void block_matvec(const float* M, const float* acc, f
     __syncthreads();
 }
 
-constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;  // a bounded wait gives up after 250 ms
-
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-__device__ __forceinline__ int ld_acquire(const int* p) {
-    int v;
-    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ unsigned long long ld_pair(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.b64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(int* p, int v) {
-    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_pair(unsigned long long* p, unsigned tag, float v) {
+    const unsigned long long w = ((unsigned long long)tag << 32) | (unsigned long long)__float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, int src_bytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Lane 0 of the calling warp polls flag f (bounded by kWaitLimitNs); the warp
-// then proceeds together.  false: the wait gave up or another CTA aborted
-// (err set).
-__device__ __forceinline__ bool warp_wait_flag(const int* f, int* err) {
-    int ok = 1;
-    if ((threadIdx.x & 31) == 0) {
-        ok = 0;
-        const unsigned long long t0 = global_ns();
-        for (;;) {
-            if (ld_acquire(f) != 0) {
-                ok = 1;
-                break;
+// The published values of source tile K (pairs pub[(K*g + q)*SB + i]) into
+// ybuf[i*NR + q]; all threads poll their own entries.  false (CTA-uniform):
+// a wait gave up (now or in another CTA).
+template <int NR>
+__device__ bool fetch_tile(const unsigned long long* __restrict__ pub, int K, int g, int kbK, unsigned tag,
+                           float* ybuf, int* err) {
+    bool ok = true;
+    for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
+        const int q = idx / SB, i = idx - q * SB;
+        float v = 0.0f;
+        if (q < g && i < kbK && ok) {
+            const unsigned long long* src = pub + ((size_t)K * g + q) * SB + i;
+            unsigned long long w = ld_pair(src);
+            if ((unsigned)(w >> 32) != tag) {
+                const unsigned long long t0 = global_ns();
+                for (;;) {
+                    __nanosleep(32);
+                    w = ld_pair(src);
+                    if ((unsigned)(w >> 32) == tag) break;
+                    if (*(volatile int*)err != 0) {
+                        ok = false;
+                        break;
+                    }
+                    if (global_ns() - t0 > kWaitLimitNs) {
+                        atomicExch(err, 1);
+                        ok = false;
+                        break;
+                    }
+                }
             }
-            if (*(volatile int*)err != 0) break;
-            if (global_ns() - t0 > kWaitLimitNs) {
-                atomicExch(err, 1);
-                break;
-            }
-            __nanosleep(64);
+            v = __uint_as_float((unsigned)w);
         }
+        ybuf[i * NR + q] = v;
     }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    __syncwarp();
-    return ok != 0;
+    return __syncthreads_and(ok) != 0;
 }
 
-// The persistent sweep.  FWD: tiles ascend, acc_j = b_j + sum_{K<j} y_K S[K][j],
-// y_j = Y_j^T acc_j -> w (ldw).  Backward: tiles descend,
-// acc_j = y_j + sum_{K>j} s_K S[K][j], s_j = X_j^T acc_j -> w (ldw), x_j = -s_j -> out.
-// in: b (forward) / y (backward), leading dimension ldi.
+// One sweep (see the file comment).  FWD: in = b (rows of ldb), out: the
+// published y.  Backward: in = the forward sweep's published y, out: x = -s
+// into xout (rows of ldb) and the published s.  g = right-hand sides of this
+// launch (<= NR).  stall (tests only): the forward sweep's second tile waits
+// for a tag that is never written, so its bounded wait runs out.
 template <int NR, bool FWD>
-__global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, int lda, int n,
-                                                   const float* __restrict__ inv, const float* __restrict__ in,
-                                                   int ldi, const float* __restrict__ wprev, float* __restrict__ w,
-                                                   int ldw, float* __restrict__ out, int ldo, int nrhs,
-                                                   int* __restrict__ flags, int* __restrict__ ticket,
-                                                   int* __restrict__ err, const int* __restrict__ never) {
+__global__ void __launch_bounds__(GT, 1)
+    k_gesl_sweep(const float* __restrict__ a, int lda, int n, const float* __restrict__ bin, float* __restrict__ xout,
+                 int ldb, unsigned long long* __restrict__ pub, int g, int* __restrict__ ticket,
+                 int* __restrict__ err, int stall) {
     extern __shared__ __align__(16) float smem[];
-    float* op = smem;                 // 128 x 128 block operator
-    float* red = op + BLK2;           // 8 x NR x 128 partial sums
-    float* acc = red + 8 * NR * SB;   // NR x 128
-    float* part = acc + NR * SB;      // 2 x NR x 128
-    float* res = part + 2 * NR * SB;  // NR x 128
+    float* op = smem;                            // 128 x 128 operator of the tile (Y or X)
+    float* scr = op + BLK2;                      // inverse scratch, later the reductions
+    float* ring = scr + kInvScratch;             // STAGES x 32 x 128 factor rows
+    float* ybuf = ring + STAGES * STAGE_FLOATS;  // 128 x NR published values of one source tile
     __shared__ int s_tile;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int nblk = (n + SB - 1) / SB;
+    const unsigned tag = FWD ? kTagFwd : kTagBwd;
+    const int c = tid & (SB - 1), h = tid >> 7;  // compute mapping: column c, rows 16h..16h+15 of a stage
     for (;;) {
         __syncthreads();  // the previous tile's shared data is consumed
         if (tid == 0) s_tile = atomicAdd(ticket, 1);
@@ -250,75 +281,94 @@ __global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, 
         if (t >= nblk) break;
         const int j = FWD ? t : nblk - 1 - t;
         const int c0 = j * SB, kb = min(SB, n - c0);
-        // the tile's block operator (Y for the forward sweep, X backward), 16-byte copies
-        {
-            const float* src = inv + (size_t)j * 2 * BLK2 + (FWD ? BLK2 : 0);
-            for (int idx = tid; idx < BLK2 / 4; idx += GT) {
-                const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(op + 4 * idx));
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 4 * idx) : "memory");
-            }
-            asm volatile("cp.async.commit_group;\n" ::: "memory");
-        }
-        // partial sums of this thread: columns c0 + 4 lane .. +3, rows 16 warp .. +15 of every source tile
-        float p[NR][4];
-#pragma unroll
-        for (int q = 0; q < NR; q++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) p[q][e] = 0.0f;
-        const int col = c0 + 4 * lane;
-        const bool vec = col + 3 < n;
-        bool ok = true;
         const int nsrc = FWD ? j : nblk - 1 - j;
-        for (int s = 0; s < nsrc; s++) {
-            const int K = FWD ? s : nblk - 1 - s;
-            const int k0 = K * SB, kbK = min(SB, n - k0);
-            float4 v[16];
+        const int total = nsrc * SPT;
+        // stage s: rows [32 (s % SPT), +32) of source tile K(s / SPT), columns [c0, c0 + 128)
+        auto issue = [&](int s) {
+            const int si = s / SPT, sr = s - si * SPT;
+            const int K = FWD ? si : nblk - 1 - si;
+            const int r0 = K * SB + sr * RS;
+            float* dst = ring + (s % STAGES) * STAGE_FLOATS;
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                const int row = 16 * warp + r;
-                const float* src = a + (size_t)(k0 + row) * lda + col;
-                if (row < kbK && vec) {
-                    v[r] = *reinterpret_cast<const float4*>(src);
+            for (int it = 0; it < STAGE_FLOATS / 4 / GT; it++) {
+                const int idx = tid + it * GT;
+                const int r = idx >> 5, cc = (idx & 31) * 4;
+                const int rem = n - (c0 + cc);  // columns left in the row: a ragged last float4 is zero-filled
+                const int bytes = (r0 + r < n && rem > 0) ? (rem >= 4 ? 16 : 4 * rem) : 0;
+                const float* src = bytes > 0 ? a + (size_t)(r0 + r) * lda + c0 + cc : a;
+                cp_async16(dst + r * SB + cc, src, bytes);
+            }
+        };
+#pragma unroll
+        for (int s = 0; s < STAGES - 1; s++) {
+            if (s < total) issue(s);
+            cp_commit();
+        }
+        // the tile's operator, while the first stages load
+        const float* d = a + (size_t)c0 * lda + c0;
+        if (FWD) {
+            inv_left_strip(d, lda, kb, 0, scr, op);
+            inv_left_strip(d, lda, kb, IST, scr, op);
+        } else {
+            inv_top_strip(d, lda, kb, 0, scr, op);
+            inv_top_strip(d, lda, kb, IST, scr, op);
+        }
+        float p[NR];
+#pragma unroll
+        for (int q = 0; q < NR; q++) p[q] = 0.0f;
+        bool ok = *(volatile int*)err == 0;
+        ok = __syncthreads_and(ok) != 0;
+        for (int s = 0; s < total && ok; s++) {
+            const int si = s / SPT, sr = s - si * SPT;
+            const int K = FWD ? si : nblk - 1 - si;
+            if (sr == 0) {
+                __syncthreads();  // every thread is done with the previous source's values
+                const bool never = FWD && stall != 0 && j == 1 && K == 0;
+                ok = fetch_tile<NR>(pub, K, g, min(SB, n - K * SB), never ? kTagNever : tag, ybuf, err);
+                if (!ok) break;
+            }
+            cp_wait<STAGES - 2>();
+            __syncthreads();
+            if (s + STAGES - 1 < total) issue(s + STAGES - 1);
+            cp_commit();
+            const float* stg = ring + (s % STAGES) * STAGE_FLOATS;
+#pragma unroll
+            for (int r = 0; r < RS / 2; r++) {
+                const int row = h * (RS / 2) + r;
+                const float v = stg[row * SB + c];
+                const float* y = ybuf + (sr * RS + row) * NR;
+                if constexpr (NR % 4 == 0) {
+#pragma unroll
+                    for (int q = 0; q < NR; q += 4) {
+                        const float4 y4 = *reinterpret_cast<const float4*>(y + q);
+                        p[q] = fmaf(y4.x, v, p[q]);
+                        p[q + 1] = fmaf(y4.y, v, p[q + 1]);
+                        p[q + 2] = fmaf(y4.z, v, p[q + 2]);
+                        p[q + 3] = fmaf(y4.w, v, p[q + 3]);
+                    }
                 } else {
-                    v[r].x = (row < kbK && col < n) ? src[0] : 0.0f;
-                    v[r].y = (row < kbK && col + 1 < n) ? src[1] : 0.0f;
-                    v[r].z = (row < kbK && col + 2 < n) ? src[2] : 0.0f;
-                    v[r].w = (row < kbK && col + 3 < n) ? src[3] : 0.0f;
-                }
-            }
-            // never (tests only): the second tile waits on a word that nothing sets
-            if (!warp_wait_flag((never != nullptr && t == 1 && s == 0) ? never : &flags[K], err)) {
-                ok = false;
-                break;
-            }
 #pragma unroll
-            for (int r = 0; r < 16; r++) {
-                const int row = 16 * warp + r;
-#pragma unroll
-                for (int q = 0; q < NR; q++) {
-                    // written by another CTA after this CTA may have cached the line: read through L2
-                    const float yk = (q < nrhs && row < kbK) ? __ldcg(wprev + (size_t)q * ldw + k0 + row) : 0.0f;
-                    p[q][0] = fmaf(yk, v[r].x, p[q][0]);
-                    p[q][1] = fmaf(yk, v[r].y, p[q][1]);
-                    p[q][2] = fmaf(yk, v[r].z, p[q][2]);
-                    p[q][3] = fmaf(yk, v[r].w, p[q][3]);
+                    for (int q = 0; q < NR; q++) p[q] = fmaf(y[q], v, p[q]);
                 }
             }
         }
-        ok = __syncthreads_and(ok);
+        cp_wait<0>();
+        ok = __syncthreads_and(ok) != 0;
+        // acc = in + the two half sums; res = operator^T acc
+        float* red = scr;                 // 2 x NR x 128
+        float* acc = red + 2 * NR * SB;   // NR x 128
+        float* part = acc + NR * SB;      // 2 x NR x 128
+        float* res = part + 2 * NR * SB;  // NR x 128
 #pragma unroll
-        for (int q = 0; q < NR; q++)
-#pragma unroll
-            for (int e = 0; e < 4; e++) red[(warp * NR + q) * SB + 4 * lane + e] = p[q][e];
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        for (int q = 0; q < NR; q++) red[(h * NR + q) * SB + c] = p[q];
         __syncthreads();
         for (int idx = tid; idx < NR * SB; idx += GT) {
             const int q = idx / SB, i = idx - q * SB;
             float v = 0.0f;
-            if (q < nrhs && i < kb) {
-                v = in[(size_t)q * ldi + c0 + i];
-#pragma unroll
-                for (int ww = 0; ww < GT / 32; ww++) v += red[(ww * NR + q) * SB + i];
+            if (q < g && i < kb) {
+                const float x0 = FWD ? bin[(size_t)q * ldb + c0 + i]
+                                     : __uint_as_float((unsigned)__ldcg(pub + ((size_t)j * g + q) * SB + i));
+                v = x0 + red[q * SB + i] + red[(NR + q) * SB + i];
             }
             acc[idx] = v;
         }
@@ -326,47 +376,41 @@ __global__ void __launch_bounds__(GT) k_gesl_sweep(const float* __restrict__ a, 
         block_matvec<NR>(op, acc, part, res);
         for (int idx = tid; idx < NR * SB; idx += GT) {
             const int q = idx / SB, i = idx - q * SB;
-            if (q < nrhs && i < kb) {
+            if (q < g && i < kb) {
                 const float v = ok ? res[idx] : __int_as_float(0x7fc00000);  // NaN marks an aborted solve
-                w[(size_t)q * ldw + c0 + i] = v;
-                if (!FWD) out[(size_t)q * ldo + c0 + i] = -v;
+                if (!FWD) xout[(size_t)q * ldb + c0 + i] = -v;
+                st_pair(pub + ((size_t)j * g + q) * SB + i, tag, v);
             }
         }
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) st_release(&flags[j], 1);
     }
 }
 
 template <int NR>
 constexpr size_t sweep_smem() {
-    return sizeof(float) * ((size_t)BLK2 + (8 * NR + 4 * NR) * (size_t)SB);
+    return sizeof(float) * ((size_t)BLK2 + kInvScratch + (size_t)STAGES * STAGE_FLOATS + (size_t)NR * SB);
 }
+// the reductions fit in the inverse scratch
+static_assert(6 * 16 * SB <= kInvScratch, "reduction buffers exceed the scratch");
+static_assert(sweep_smem<16>() <= 227 * 1024, "sweep shared memory");
 
 template <int NR>
-int sweeps(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* w1, float* w2, const float* inv,
-           int* sync, int* err, bool stall, int sms, cudaStream_t st) {
+int sweeps(const float* a, int lda, int n, float* b, int ldb, int g, unsigned long long* pub, int* tickets, int* err,
+           bool stall, int sms, cudaStream_t st) {
     const int nblk = (n + SB - 1) / SB;
-    int* flags_f = sync;
-    int* flags_b = sync + nblk;
-    int* tickets = sync + 2 * nblk;
-    const int* never = stall ? tickets + 2 : nullptr;
-    LP_CUDA(cudaMemsetAsync(sync, 0, sizeof(int) * gesl_sync_ints(n), st));  // err is the caller's
-    const int per_sm = NR >= 16 ? 1 : 2;
-    const int grid = std::min(nblk, per_sm * sms);
-    // forward: b -> y (w2)
-    k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, b, ldb, w2, w2, n, nullptr, 0, nrhs,
-                                                              flags_f, tickets, err, never);
-    // backward: y (w2) -> s (w1), x -> b
-    k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, inv, w2, n, w1, w1, n, b, ldb, nrhs,
-                                                               flags_b, tickets + 1, err, nullptr);
+    const int grid = std::min(nblk, sms);
+    LP_CUDA(cudaMemsetAsync(tickets, 0, 2 * sizeof(int), st));
+    LP_CUDA(cudaMemsetAsync(pub, 0, sizeof(unsigned long long) * (size_t)nblk * SB * g, st));
+    k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, b, nullptr, ldb, pub, g, tickets, err,
+                                                               stall ? 1 : 0);
+    k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, nullptr, b, ldb, pub, g, tickets + 1, err,
+                                                                0);
     count_launch(2);
     LP_CUDA(cudaGetLastError());
     return LP_OK;
 }
 
 template <int NR>
-int inv_attrs() {
+int sweep_attrs() {
     LP_CUDA(cudaFuncSetAttribute(k_gesl_sweep<NR, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sweep_smem<NR>()));
     LP_CUDA(cudaFuncSetAttribute(k_gesl_sweep<NR, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -377,39 +421,25 @@ int inv_attrs() {
 }  // namespace
 
 int gesl_inv_init_attrs() {
-    LP_CUDA(cudaFuncSetAttribute(k_inv_top, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvTopSmem));
-    LP_CUDA(cudaFuncSetAttribute(k_inv_left, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvLeftSmem));
-    LP_CHECK(inv_attrs<1>());
-    LP_CHECK(inv_attrs<4>());
-    LP_CHECK(inv_attrs<16>());
+    LP_CHECK(sweep_attrs<1>());
+    LP_CHECK(sweep_attrs<4>());
+    LP_CHECK(sweep_attrs<16>());
     return LP_OK;
 }
 
-size_t gesl_inv_floats(int n) { return (size_t)((n + SB - 1) / SB) * 2 * BLK2; }
-
-// X and Y of every diagonal block of the factors (inv: gesl_inv_floats(n)).
-int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_t st) {
-    const int nblk = (n + SB - 1) / SB;
-    if (nblk > 65535) return fail(LP_E_INVALID, "gesl: too many blocks");
-    const dim3 grid(SB / IST, nblk);
-    k_inv_top<<<grid, 256, kInvTopSmem, st>>>(a, lda, n, inv);
-    k_inv_left<<<grid, 256, kInvLeftSmem, st>>>(a, lda, n, inv);
-    count_launch(2);
-    LP_CUDA(cudaGetLastError());
-    return LP_OK;
+// Published-value pairs of one solve: ceil(n / 128) * 128 * min(nrhs, 16).
+size_t gesl_pub_pairs(int n, int nrhs) {
+    const size_t g = nrhs < 16 ? nrhs : 16;
+    return (size_t)((n + SB - 1) / SB) * SB * g;
 }
 
-// Sync words of the persistent sweeps: flags of both directions, two tickets,
-// and one word that nothing sets (the target of the test stall).
-size_t gesl_sync_ints(int n) { return 2 * (size_t)((n + SB - 1) / SB) + 3; }
-
-// Forward + back substitution with precomputed block inverses; sync:
-// gesl_sync_ints(n) ints (cleared here); err: an error word the caller zeroes
-// and reads (set when a bounded wait gave up; that tile is written as NaN).
-// stall (tests only): the forward sweep's second tile waits on a word that
-// nothing sets, so its bounded wait runs out.
-int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
-                    int* sync, int* err, bool stall, cudaStream_t st) {
+// Forward + back substitution for nrhs rows of b (overwritten by x), in
+// chunks of at most 16 right-hand sides.  pub: gesl_pub_pairs(n, nrhs) pairs;
+// tickets: 2 ints; err: an error word the caller zeroes and reads (set when a
+// bounded wait gave up; that tile is written as NaN).  pub and tickets are
+// cleared here before every chunk.  stall (tests only): see k_gesl_sweep.
+int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, unsigned long long* pub,
+                    int* tickets, int* err, bool stall, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return LP_OK;
     if (lda % 4 != 0 || !aligned16(a)) return fail(LP_E_INVALID, "gesl: factors need lda % 4 == 0, 16-byte aligned");
     int dev = 0, sms = 0;
@@ -418,14 +448,13 @@ int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs,
     for (int r0 = 0; r0 < nrhs; r0 += 16) {
         const int g = (nrhs - r0) < 16 ? (nrhs - r0) : 16;
         float* bb = b + (size_t)r0 * ldb;
-        float* w1 = work;
-        float* w2 = work + (size_t)n * g;
+        const bool stall_here = stall && r0 == 0;
         if (g == 1)
-            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
+            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
         else if (g <= 4)
-            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
+            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
         else
-            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, w1, w2, inv, sync, err, stall && r0 == 0, sms, st));
+            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
     }
     return LP_OK;
 }

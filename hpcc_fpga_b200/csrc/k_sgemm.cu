@@ -10,7 +10,11 @@
 // Both operands are k-major, so every tile load is a run of 16-byte cp.async
 // copies into a STAGES-deep shared-memory ring.  128 x 128 x 16 tiles, 256
 // threads, 8 x 8 FP32 accumulators per thread (two 4-row and two 4-column
-// groups, conflict-free float4 shared loads), FFMA on the FP32 pipe.  C is
+// groups, conflict-free float4 shared loads), held as 8 x 4 pairs and updated
+// with Blackwell's packed FP32 FMA (FFMA2, fma.rn.f32x2: two independent
+// correctly rounded fused multiply-adds per issued instruction, so each
+// element is computed exactly as fmaf would).  One FFMA2 per pair halves the
+// FMA instructions of the FFMA form, whose issue rate was the limit.  C is
 // read and written once per launch.
 #include "lp_common.cuh"
 
@@ -52,11 +56,12 @@ __global__ void __launch_bounds__(NT, 2) k_sgemm_update(float* __restrict__ C, i
         }
     };
 
-    float acc[8][8];
+    // acc[i][h] holds the pair of columns (2h, 2h + 1) of row i of the thread's 8 x 8 tile
+    float2 acc[8][4];
 #pragma unroll
     for (int i = 0; i < 8; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+        for (int j = 0; j < 4; j++) acc[i][j] = make_float2(0.0f, 0.0f);
 
     const int KT = K / BK;
 #pragma unroll
@@ -79,11 +84,14 @@ __global__ void __launch_bounds__(NT, 2) k_sgemm_update(float* __restrict__ C, i
             const float4 b0 = *reinterpret_cast<const float4*>(&bsm[k * BN + tx * 4]);
             const float4 b1 = *reinterpret_cast<const float4*>(&bsm[k * BN + 64 + tx * 4]);
             const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-            const float b[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+            const float2 b[4] = {make_float2(b0.x, b0.y), make_float2(b0.z, b0.w), make_float2(b1.x, b1.y),
+                                 make_float2(b1.z, b1.w)};
 #pragma unroll
-            for (int i = 0; i < 8; i++)
+            for (int i = 0; i < 8; i++) {
+                const float2 ai = make_float2(a[i], a[i]);
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; j++) acc[i][j] = __ffma2_rn(ai, b[j], acc[i][j]);
+            }
         }
     }
     cp_async_wait<0>();
@@ -98,10 +106,10 @@ __global__ void __launch_bounds__(NT, 2) k_sgemm_update(float* __restrict__ C, i
             if (c >= N) continue;
             float4* p = reinterpret_cast<float4*>(C + (size_t)r * ldc + c);
             float4 v = *p;
-            v.x += acc[i][h * 4 + 0];
-            v.y += acc[i][h * 4 + 1];
-            v.z += acc[i][h * 4 + 2];
-            v.w += acc[i][h * 4 + 3];
+            v.x += acc[i][2 * h].x;
+            v.y += acc[i][2 * h].y;
+            v.z += acc[i][2 * h + 1].x;
+            v.w += acc[i][2 * h + 1].y;
             *p = v;
         }
     }

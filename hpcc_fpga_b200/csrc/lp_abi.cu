@@ -448,18 +448,15 @@ int gefa_f32_streamed(lp_ctx* c, const float* hA, float* dA, int n, int lda, int
 }
 
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st) {
-    const size_t wf = gesl_work_floats(n, nrhs), si = gesl_sync_ints(n);
-    LP_CHECK(c->gw.ensure(sizeof(float) * wf + sizeof(int) * si));
-    LP_CHECK(c->ginv.ensure(sizeof(float) * gesl_inv_floats(n)));
+    const size_t pairs = gesl_pub_pairs(n, nrhs);
+    LP_CHECK(c->gw.ensure(sizeof(unsigned long long) * pairs + 4 * sizeof(int)));
     LP_CHECK(c->gerr.ensure(sizeof(int)));
-    float* inv = static_cast<float*>(c->ginv.ptr);
-    float* work = static_cast<float*>(c->gw.ptr);
-    int* sync = reinterpret_cast<int*>(work + wf);
+    auto* pub = static_cast<unsigned long long*>(c->gw.ptr);
+    int* tickets = reinterpret_cast<int*>(pub + pairs);
     const bool stall = c->stall_site == LP_STALL_GESL;
     c->stall_site = stall ? 0 : c->stall_site;
     const int e = prof_begin(c, st);
-    LP_CHECK(launch_diag_inverses(dLU, lda, n, inv, st));
-    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, work, inv, sync, static_cast<int*>(c->gerr.ptr), stall, st));
+    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, pub, tickets, static_cast<int*>(c->gerr.ptr), stall, st));
     const double nn = n;
     return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
 }
@@ -541,7 +538,6 @@ int lp_ctx_create(int device, lp_ctx** out) {
     LP_CHECK(lu_init_attrs());
     LP_CHECK(trsm_init_attrs());
     LP_CHECK(sgemm_init_attrs());
-    LP_CHECK(gesl_init_attrs());
     LP_CHECK(gesl_inv_init_attrs());
     LP_CHECK(umma_init_attrs());
     LP_CHECK(batch_init_attrs());

@@ -105,15 +105,13 @@ int launch_dgemm_update(double* c, int ldc, const double* lt, int ldlt, const do
 int dgemm_init_attrs();
 int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t s);
 int launch_transpose_f64(const double* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t s);
-// Forward + back substitution for nrhs rows of b (see k_gesl.cu).
-int launch_gesl(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, cudaStream_t s);
-size_t gesl_work_floats(int n, int nrhs);
-// The same with precomputed inverses of the 128 x 128 diagonal blocks (k_gesl_inv.cu).
-int launch_diag_inverses(const float* a, int lda, int n, float* inv, cudaStream_t s);
-int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, float* work, const float* inv,
-                    int* sync, int* err, bool stall, cudaStream_t st);
-size_t gesl_sync_ints(int n);
-size_t gesl_inv_floats(int n);
+// Forward + back substitution for nrhs rows of b with the encoded factors:
+// two persistent sweeps per 16 right-hand sides, each CTA inverting its own
+// diagonal block (k_gesl_inv.cu).  pub: gesl_pub_pairs(n, nrhs) 64-bit words,
+// tickets: 2 ints, err: an error word the caller zeroes and reads.
+int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, unsigned long long* pub,
+                    int* tickets, int* err, bool stall, cudaStream_t st);
+size_t gesl_pub_pairs(int n, int nrhs);
 int gesl_inv_init_attrs();
 // FP64 refinement pieces (see k_ir.cu).
 int launch_residual_f64(const float* a, int lda, int n, const double* x, int ldx, const double* b, int ldb,
@@ -128,6 +126,5 @@ int launch_f32_to_f64(double* y, const float* v, size_t n, cudaStream_t s);
 int lu_init_attrs();
 int trsm_init_attrs();
 int sgemm_init_attrs();
-int gesl_init_attrs();
 
 }  // namespace lp

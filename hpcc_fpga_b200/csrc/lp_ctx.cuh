@@ -130,8 +130,7 @@ struct lp_ctx {
     lp::Workspace err;   // device error word of the tensor-core update (bounded waits)
     lp::Workspace tri;   // mixed panel: inverses of the diagonal block's triangles (2 x bs x bs) + Lt scratch
     lp::Workspace tq;    // mixed panel: split-BF16 operands of the top and left products
-    lp::Workspace gw;    // substitution work vectors
-    lp::Workspace ginv;  // inverses of the 128 x 128 diagonal blocks of the factors (substitution)
+    lp::Workspace gw;    // substitution: published values of the sweeps (64-bit pairs) and their tickets
     lp::Workspace gerr;  // error word of the substitution sweeps (non-zero: a bounded wait gave up)
     int* hstat = nullptr;                     // pinned host copy of an error word
     int stall_site = 0;                       // lp_ctx_test_stall: the next wait of this site never completes
@@ -163,7 +162,7 @@ struct lp_ctx {
     double prof_s[LP_NSTAGES] = {0}, prof_flops[LP_NSTAGES] = {0}, prof_bytes[LP_NSTAGES] = {0};
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
-        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &ginv, &gerr, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
+        lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &gerr, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
                                 &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);

@@ -217,14 +217,17 @@ int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nr
  * cudaFree — code that hands all device memory to its own pool, code that
  * records CUDA graphs or runs inside a latency-bound serving loop (where an
  * allocation can synchronize the device), or a plugin host that forbids it.
- * This entry point allocates nothing and needs no lp_ctx: its two work vectors
- * live in one fixed device array of 2^20 floats (4 MiB) that every GPU which
- * loads the library holds until the process exits, so it accepts only
- * 2 * n * min(nrhs, 16) <= 1048576 and returns LP_E_INVALID beyond that.
- * It runs the blocked substitution kernels k_gesl_fwd / k_gesl_bwd (one
- * launch per 128-row block and direction, no inverses of the diagonal blocks)
- * rather than lp_gesl_dev's persistent sweeps, whose inverses would need
- * more scratch; the results agree to FP32 rounding.
+ * This entry point allocates nothing and needs no lp_ctx.  It runs the same
+ * two persistent sweeps as lp_gesl_dev, whose only global scratch is the
+ * array of values the sweeps publish to one another (one 64-bit word per
+ * unknown and right-hand side of a 16-wide chunk); here that array is one
+ * fixed device array of 2^19 words (4 MiB, plus 16 bytes of counters) that
+ * every GPU which loads the library holds until the process exits, so it
+ * accepts only ceil(n / 128) * 128 * min(nrhs, 16) <= 524288 (n <= 32768 with
+ * 16 or more right-hand sides, n <= 524288 with one) and returns LP_E_INVALID
+ * beyond that.  Unlike lp_gesl_dev it does not wait for the device, so it
+ * cannot report a bounded wait of the sweeps that ran out: the affected
+ * solution entries are then NaN.
  * The first call on a device (the current device) looks up the array's
  * address and sets kernel attributes for that device; make that first call
  * before any stream capture.  The address is looked up in, and cached for, the

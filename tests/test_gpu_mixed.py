@@ -194,6 +194,7 @@ def test_mixed_large_blocks_margin_sweep(ctx, dev, seeded_systems, seed, bs):
         dB64 = set_margin(torch, dA0, n, margin)
         for prec in ("bf16", "fp8"):
             dLU = dA0.clone()
+            torch.cuda.synchronize()  # torch's stream and the library's stream are not ordered
             ctx.gefa_prec(prec, dLU.data_ptr(), n, n, bs)
             dX = dev.empty((n,), np.float64)
             t = ctx.refine(dA0.data_ptr(), n, dLU.data_ptr(), n, dB64.data_ptr(), dX.data_ptr(), 1, 50)
