@@ -19,10 +19,11 @@
 // ticket order (forward 0, 1, 2, ...; backward from the last tile down) and,
 // for its tile j:
 //   1. starts streaming the factor blocks S[K][j] of every source tile K
-//      (forward K < j, backward K > j) through a 5-stage cp.async ring of
-//      32-row stages, so a whole source tile plus one stage is in flight;
-//   2. meanwhile inverts its own diagonal block into shared memory (Y or X:
-//      no separate launch, no global workspace for the operators);
+//      (forward K < j, backward K > j) through a cp.async ring of 32-row
+//      stages (5 to 7 deep), so a whole source tile and more is in flight;
+//   2. inverts its own diagonal block into shared memory (Y or X: no
+//      separate launch, no global workspace for the operators) when it
+//      would otherwise wait for a source that is not published yet;
 //   3. for each source tile waits for its published values (one poll loop
 //      over the tile's (value, tag) pairs), then adds its contributions;
 //   4. forms acc_j, multiplies by the operator, publishes its own values.
@@ -52,7 +53,6 @@ constexpr int IST = 64;        // strip width of the inverse recurrences
 constexpr int BLK2 = SB * SB;  // floats per operator
 constexpr int RS = 32;         // factor rows per ring stage
 constexpr int SPT = SB / RS;   // stages per source tile
-constexpr int STAGES = SPT + 1;
 constexpr int STAGE_FLOATS = RS * SB;
 constexpr int kInvTopScratch = SB * IST + SB * ICH;
 constexpr int kInvLeftScratch = IST * (SB + 1) + ICH * SB;
@@ -169,31 +169,6 @@ __device__ void inv_left_strip(const float* __restrict__ d, int lda, int kb, int
     __syncthreads();
 }
 
-// coef[r][i] = sum_k M[k][i] * acc[r][k] for a 128 x 128 operator M (shared
-// memory); all 256 threads: thread (h, i) sums k in [64h, 64h+64).
-template <int NR>
-__device__ __forceinline__ void block_matvec(const float* M, const float* acc, float* part, float* coef) {
-    const int i = threadIdx.x & (SB - 1), h = threadIdx.x >> 7;
-    float p[NR];
-#pragma unroll
-    for (int r = 0; r < NR; r++) p[r] = 0.0f;
-#pragma unroll 16
-    for (int kk = 0; kk < SB / 2; kk++) {
-        const int k = h * (SB / 2) + kk;
-        const float m = M[k * SB + i];
-#pragma unroll
-        for (int r = 0; r < NR; r++) p[r] = fmaf(m, acc[r * SB + k], p[r]);
-    }
-#pragma unroll
-    for (int r = 0; r < NR; r++) part[(h * NR + r) * SB + i] = p[r];
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
-        const int r = idx / SB, ii = idx - r * SB;
-        coef[idx] = part[r * SB + ii] + part[(NR + r) * SB + ii];
-    }
-    __syncthreads();
-}
-
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -216,39 +191,79 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// The published values of source tile K (pairs pub[(K*g + q)*SB + i]) into
-// ybuf[i*NR + q]; all threads poll their own entries.  false (CTA-uniform):
-// a wait gave up (now or in another CTA).
+// Ring depth per right-hand-side width: as deep as shared memory allows
+// (227 KB per CTA) beside the operator, the inverse scratch and the staged
+// values.
 template <int NR>
-__device__ bool fetch_tile(const unsigned long long* __restrict__ pub, int K, int g, int kbK, unsigned tag,
-                           float* ybuf, int* err) {
-    bool ok = true;
-    for (int idx = threadIdx.x; idx < NR * SB; idx += GT) {
+__host__ __device__ constexpr int stages() {
+    return NR == 1 ? 7 : NR <= 4 ? 6 : 5;
+}
+
+// Published values of one source tile, prefetched into registers: thread t
+// owns entries idx = t + m * GT (q = idx / 128, i = idx % 128) of the tile's
+// NR x 128 block.
+template <int NR>
+struct Pending {
+    static constexpr int M = (NR * SB + GT - 1) / GT;
+    unsigned long long w[M];
+};
+
+// Issue the relaxed loads of source tile K's pairs (entries this launch does
+// not need read as valid zeros).
+template <int NR>
+__device__ __forceinline__ void prefetch_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, int K,
+                                              int g, int kbK, unsigned tag) {
+#pragma unroll
+    for (int m = 0; m < Pending<NR>::M; m++) {
+        const int idx = threadIdx.x + m * GT;
         const int q = idx / SB, i = idx - q * SB;
-        float v = 0.0f;
-        if (q < g && i < kbK && ok) {
+        pd.w[m] = (idx < NR * SB && q < g && i < kbK) ? ld_pair(pub + ((size_t)K * g + q) * SB + i)
+                                                      : ((unsigned long long)tag << 32);
+    }
+}
+
+// true when every prefetched entry of the calling thread carries `tag`.
+template <int NR>
+__device__ __forceinline__ bool all_tagged(const Pending<NR>& pd, unsigned tag) {
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < Pending<NR>::M; m++) ok = ok && (unsigned)(pd.w[m] >> 32) == tag;
+    return ok;
+}
+
+// Complete the prefetched values of source tile K: entries not yet carrying
+// `tag` are polled (bounded by kWaitLimitNs; another CTA's error ends the
+// wait too); the values go to ybuf[i*NR + q].  false (CTA-uniform): a wait
+// gave up (here or in another CTA).
+template <int NR>
+__device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, int K, int g,
+                             unsigned tag, float* ybuf, int* err) {
+    bool ok = true;
+#pragma unroll
+    for (int m = 0; m < Pending<NR>::M; m++) {
+        const int idx = threadIdx.x + m * GT;
+        if (idx >= NR * SB) continue;
+        const int q = idx / SB, i = idx - q * SB;
+        unsigned long long w = pd.w[m];
+        if ((unsigned)(w >> 32) != tag && ok) {
             const unsigned long long* src = pub + ((size_t)K * g + q) * SB + i;
-            unsigned long long w = ld_pair(src);
-            if ((unsigned)(w >> 32) != tag) {
-                const unsigned long long t0 = global_ns();
-                for (;;) {
-                    __nanosleep(32);
-                    w = ld_pair(src);
-                    if ((unsigned)(w >> 32) == tag) break;
-                    if (*(volatile int*)err != 0) {
-                        ok = false;
-                        break;
-                    }
-                    if (global_ns() - t0 > kWaitLimitNs) {
-                        atomicExch(err, 1);
-                        ok = false;
-                        break;
-                    }
+            const unsigned long long t0 = global_ns();
+            for (;;) {
+                __nanosleep(32);
+                w = ld_pair(src);
+                if ((unsigned)(w >> 32) == tag) break;
+                if (*(volatile int*)err != 0) {
+                    ok = false;
+                    break;
+                }
+                if (global_ns() - t0 > kWaitLimitNs) {
+                    atomicExch(err, 1);
+                    ok = false;
+                    break;
                 }
             }
-            v = __uint_as_float((unsigned)w);
         }
-        ybuf[i * NR + q] = v;
+        ybuf[i * NR + q] = __uint_as_float((unsigned)w);
     }
     return __syncthreads_and(ok) != 0;
 }
@@ -258,16 +273,24 @@ __device__ bool fetch_tile(const unsigned long long* __restrict__ pub, int K, in
 // into xout (rows of ldb) and the published s.  g = right-hand sides of this
 // launch (<= NR).  stall (tests only): the forward sweep's second tile waits
 // for a tag that is never written, so its bounded wait runs out.
+//
+// Per source tile the CTA completes the values it prefetched one tile ahead
+// (already published sources cost no round trip); the tile's operator is
+// computed at the first source that is not yet published (the CTA would wait
+// anyway), or at the end; the tile's input is staged into shared memory by
+// cp.async with the first ring stage.
 template <int NR, bool FWD>
 __global__ void __launch_bounds__(GT, 1)
     k_gesl_sweep(const float* __restrict__ a, int lda, int n, const float* __restrict__ bin, float* __restrict__ xout,
                  int ldb, unsigned long long* __restrict__ pub, int g, int* __restrict__ ticket,
                  int* __restrict__ err, int stall) {
+    constexpr int STG = stages<NR>();
     extern __shared__ __align__(16) float smem[];
-    float* op = smem;                            // 128 x 128 operator of the tile (Y or X)
-    float* scr = op + BLK2;                      // inverse scratch, later the reductions
-    float* ring = scr + kInvScratch;             // STAGES x 32 x 128 factor rows
-    float* ybuf = ring + STAGES * STAGE_FLOATS;  // 128 x NR published values of one source tile
+    float* op = smem;                         // 128 x 128 operator of the tile (Y or X)
+    float* scr = op + BLK2;                   // inverse scratch, later the reductions
+    float* ring = scr + kInvScratch;          // STG x 32 x 128 factor rows
+    float* ybuf = ring + STG * STAGE_FLOATS;  // 128 x NR published values of one source tile
+    float* inb = ybuf + NR * SB;              // NR x 128 input of the tile (b_j or y_j)
     __shared__ int s_tile;
     const int tid = threadIdx.x;
     const int nblk = (n + SB - 1) / SB;
@@ -288,7 +311,7 @@ __global__ void __launch_bounds__(GT, 1)
             const int si = s / SPT, sr = s - si * SPT;
             const int K = FWD ? si : nblk - 1 - si;
             const int r0 = K * SB + sr * RS;
-            float* dst = ring + (s % STAGES) * STAGE_FLOATS;
+            float* dst = ring + (s % STG) * STAGE_FLOATS;
 #pragma unroll
             for (int it = 0; it < STAGE_FLOATS / 4 / GT; it++) {
                 const int idx = tid + it * GT;
@@ -299,39 +322,47 @@ __global__ void __launch_bounds__(GT, 1)
                 cp_async16(dst + r * SB + cc, src, bytes);
             }
         };
+        // the tile's input: b_j (forward) or the forward sweep's y_j (the low word of its pairs)
+        for (int idx = tid; idx < NR * SB; idx += GT) {
+            const int q = idx / SB, i = idx - q * SB;
+            if (q < g && i < kb) {
+                const float* src = FWD ? bin + (size_t)q * ldb + c0 + i
+                                       : reinterpret_cast<const float*>(pub + ((size_t)j * g + q) * SB + i);
+                cp_async4(inb + idx, src);
+            } else {
+                inb[idx] = 0.0f;
+            }
+        }
 #pragma unroll
-        for (int s = 0; s < STAGES - 1; s++) {
+        for (int s = 0; s < STG - 1; s++) {
             if (s < total) issue(s);
             cp_commit();
         }
-        // the tile's operator, while the first stages load
         const float* d = a + (size_t)c0 * lda + c0;
-        if (FWD) {
-            inv_left_strip(d, lda, kb, 0, scr, op);
-            inv_left_strip(d, lda, kb, IST, scr, op);
-        } else {
-            inv_top_strip(d, lda, kb, 0, scr, op);
-            inv_top_strip(d, lda, kb, IST, scr, op);
-        }
+        auto invert = [&]() {
+            if (FWD) {
+                inv_left_strip(d, lda, kb, 0, scr, op);
+                inv_left_strip(d, lda, kb, IST, scr, op);
+            } else {
+                inv_top_strip(d, lda, kb, 0, scr, op);
+                inv_top_strip(d, lda, kb, IST, scr, op);
+            }
+        };
+        bool inverted = false;
         float p[NR];
 #pragma unroll
         for (int q = 0; q < NR; q++) p[q] = 0.0f;
         bool ok = *(volatile int*)err == 0;
         ok = __syncthreads_and(ok) != 0;
-        for (int s = 0; s < total && ok; s++) {
-            const int si = s / SPT, sr = s - si * SPT;
-            const int K = FWD ? si : nblk - 1 - si;
-            if (sr == 0) {
-                __syncthreads();  // every thread is done with the previous source's values
-                const bool never = FWD && stall != 0 && j == 1 && K == 0;
-                ok = fetch_tile<NR>(pub, K, g, min(SB, n - K * SB), never ? kTagNever : tag, ybuf, err);
-                if (!ok) break;
-            }
-            cp_wait<STAGES - 2>();
-            __syncthreads();
-            if (s + STAGES - 1 < total) issue(s + STAGES - 1);
-            cp_commit();
-            const float* stg = ring + (s % STAGES) * STAGE_FLOATS;
+        Pending<NR> pd;
+        if (nsrc > 0 && ok) {
+            const int K0 = FWD ? 0 : nblk - 1;
+            const bool never = FWD && stall != 0 && j == 1;
+            prefetch_tile<NR>(pd, pub, K0, g, min(SB, n - K0 * SB), never ? kTagNever : tag);
+        }
+        // contributions of ring stage s (rows sr*32.. of its source tile) to this thread's sums
+        auto consume = [&](int s, int sr) {
+            const float* stg = ring + (s % STG) * STAGE_FLOATS;
 #pragma unroll
             for (int r = 0; r < RS / 2; r++) {
                 const int row = h * (RS / 2) + r;
@@ -351,33 +382,75 @@ __global__ void __launch_bounds__(GT, 1)
                     for (int q = 0; q < NR; q++) p[q] = fmaf(y[q], v, p[q]);
                 }
             }
+        };
+        for (int s = 0; s < total && ok; s++) {
+            const int si = s / SPT, sr = s - si * SPT;
+            const int K = FWD ? si : nblk - 1 - si;
+            if (sr == 0) {
+                const unsigned want = (FWD && stall != 0 && j == 1 && K == 0) ? kTagNever : tag;
+                __syncthreads();  // every thread is done with the previous source's values
+                if (!inverted && __syncthreads_and(all_tagged<NR>(pd, want)) == 0) {
+                    invert();  // this source is not published yet: the CTA would wait anyway
+                    inverted = true;
+                }
+                ok = resolve_tile<NR>(pd, pub, K, g, want, ybuf, err);
+                if (!ok) break;
+                if (si + 1 < nsrc) {
+                    const int K1 = FWD ? si + 1 : nblk - 2 - si;
+                    prefetch_tile<NR>(pd, pub, K1, g, min(SB, n - K1 * SB), tag);
+                } else {
+                    // the last source (on the chain's critical path): all of its stages are in
+                    // the ring already (STG > SPT), so one wait and one barrier cover them
+                    cp_wait<0>();
+                    __syncthreads();
+#pragma unroll
+                    for (int r4 = 0; r4 < SPT; r4++) consume(s + r4, r4);
+                    break;
+                }
+            }
+            cp_wait<STG - 2>();
+            __syncthreads();
+            if (s + STG - 1 < total) issue(s + STG - 1);
+            cp_commit();
+            consume(s, sr);
         }
         cp_wait<0>();
-        ok = __syncthreads_and(ok) != 0;
-        // acc = in + the two half sums; res = operator^T acc
-        float* red = scr;                 // 2 x NR x 128
-        float* acc = red + 2 * NR * SB;   // NR x 128
+        if (!inverted) invert();
+        // acc = in + the two half sums; res = operator^T acc; published from the two halves of the product
+        float* red = scr;                 // NR x 128: the upper half's sums
+        float* acc = red + NR * SB;       // NR x 128
         float* part = acc + NR * SB;      // 2 x NR x 128
-        float* res = part + 2 * NR * SB;  // NR x 128
+        if (h == 1) {
 #pragma unroll
-        for (int q = 0; q < NR; q++) red[(h * NR + q) * SB + c] = p[q];
-        __syncthreads();
-        for (int idx = tid; idx < NR * SB; idx += GT) {
-            const int q = idx / SB, i = idx - q * SB;
-            float v = 0.0f;
-            if (q < g && i < kb) {
-                const float x0 = FWD ? bin[(size_t)q * ldb + c0 + i]
-                                     : __uint_as_float((unsigned)__ldcg(pub + ((size_t)j * g + q) * SB + i));
-                v = x0 + red[q * SB + i] + red[(NR + q) * SB + i];
-            }
-            acc[idx] = v;
+            for (int q = 0; q < NR; q++) red[q * SB + c] = p[q];
+        }
+        ok = __syncthreads_and(ok) != 0;
+        if (h == 0) {
+#pragma unroll
+            for (int q = 0; q < NR; q++) acc[q * SB + c] = (q < g && c < kb) ? inb[q * SB + c] + p[q] + red[q * SB + c] : 0.0f;
         }
         __syncthreads();
-        block_matvec<NR>(op, acc, part, res);
+        {
+            const int i = tid & (SB - 1), hh = tid >> 7;
+            float pr[NR];
+#pragma unroll
+            for (int r = 0; r < NR; r++) pr[r] = 0.0f;
+#pragma unroll 16
+            for (int kk = 0; kk < SB / 2; kk++) {
+                const int k = hh * (SB / 2) + kk;
+                const float m = op[k * SB + i];
+#pragma unroll
+                for (int r = 0; r < NR; r++) pr[r] = fmaf(m, acc[r * SB + k], pr[r]);
+            }
+#pragma unroll
+            for (int r = 0; r < NR; r++) part[(hh * NR + r) * SB + i] = pr[r];
+        }
+        __syncthreads();
         for (int idx = tid; idx < NR * SB; idx += GT) {
             const int q = idx / SB, i = idx - q * SB;
             if (q < g && i < kb) {
-                const float v = ok ? res[idx] : __int_as_float(0x7fc00000);  // NaN marks an aborted solve
+                const float v = ok ? part[q * SB + i] + part[(NR + q) * SB + i]
+                                   : __int_as_float(0x7fc00000);  // NaN marks an aborted solve
                 if (!FWD) xout[(size_t)q * ldb + c0 + i] = -v;
                 st_pair(pub + ((size_t)j * g + q) * SB + i, tag, v);
             }
@@ -387,11 +460,13 @@ __global__ void __launch_bounds__(GT, 1)
 
 template <int NR>
 constexpr size_t sweep_smem() {
-    return sizeof(float) * ((size_t)BLK2 + kInvScratch + (size_t)STAGES * STAGE_FLOATS + (size_t)NR * SB);
+    return sizeof(float) *
+           ((size_t)BLK2 + kInvScratch + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
 }
 // the reductions fit in the inverse scratch
-static_assert(6 * 16 * SB <= kInvScratch, "reduction buffers exceed the scratch");
-static_assert(sweep_smem<16>() <= 227 * 1024, "sweep shared memory");
+static_assert(4 * 16 * SB <= kInvScratch, "reduction buffers exceed the scratch");
+static_assert(sweep_smem<1>() <= 227 * 1024 && sweep_smem<4>() <= 227 * 1024 && sweep_smem<16>() <= 227 * 1024,
+              "sweep shared memory");
 
 template <int NR>
 int sweeps(const float* a, int lda, int n, float* b, int ldb, int g, unsigned long long* pub, int* tickets, int* err,

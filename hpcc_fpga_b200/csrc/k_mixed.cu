@@ -4,9 +4,11 @@
 // triangles of the FP32 diagonal block (panel_tc).  After each panel its left block column L and top
 // block row T are rounded to the tensor-core operand type:
 //   BF16:  Lq[m][k] = bf16(L[m][k]),  Tq[n][k] = bf16(T[k][n]);
-//   E4M3:  one absmax scale per 512-row block of L and per 512-column block
-//          of T (s = absmax / 448), Lq = e4m3(L / s_L), Tq = e4m3(T^T / s_T),
-//          and the update adds s_L * s_T * (Lq Tq^T) in FP32.
+//   E4M3:  one absmax scale per 512 x 512 block: per 512-row block of L and
+//          512-wide K segment, per 512-column block of T and K segment
+//          (s = absmax / 448), Lq = e4m3(L / s_L), Tq = e4m3(T^T / s_T), and
+//          the update adds sum_seg s_L(seg) * s_T(seg) * (Lq_seg Tq_seg^T) in
+//          FP32 (k_umma.cu accumulates every segment on its own).
 // The FP32 factors the substitution uses are these rounded-update factors;
 // accuracy is recovered by FP64 iterative refinement (lp_solve.cu).
 //   BF16x6 (FP32 emulation): every element x of L and T is split exactly into
@@ -30,22 +32,30 @@ __device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
     atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));  // non-negative floats order as ints
 }
 
-// amax[r / 512] = max |L[r][0..k)| over each 512-row block.
-__global__ void k_absmax_rows(const float* __restrict__ L, int ldl, int rows, int k, float* __restrict__ amax) {
-    const int r = blockIdx.x;
+// amax[seg * nblk + r / 512] = max |L[r][512 seg .. 512 seg + 512)| over each
+// 512-row block (blockIdx.y = seg).
+__global__ void k_absmax_rows(const float* __restrict__ L, int ldl, int rows, int k, int nblk,
+                              float* __restrict__ amax) {
+    const int r = blockIdx.x, seg = blockIdx.y;
+    const int c1 = min(k, 512 * (seg + 1));
     float m = 0.0f;
-    for (int c = threadIdx.x; c < k; c += blockDim.x) m = fmaxf(m, fabsf(L[(size_t)r * ldl + c]));
+    for (int c = 512 * seg + threadIdx.x; c < c1; c += blockDim.x) m = fmaxf(m, fabsf(L[(size_t)r * ldl + c]));
     for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&amax[r >> 9], m);
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&amax[seg * nblk + (r >> 9)], m);
 }
 
-// amax[c / 512] = max |T[0..k)[c]| over each 512-column block.
-__global__ void k_absmax_cols(const float* __restrict__ T, int ldt, int k, int cols, float* __restrict__ amax) {
+// amax[seg * nblk + c / 512] = max |T[512 seg .. 512 seg + 512)[c]| over each
+// 512-column block.
+__global__ void k_absmax_cols(const float* __restrict__ T, int ldt, int k, int cols, int nblk,
+                              float* __restrict__ amax) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
-    float m = 0.0f;
-    for (int r = 0; r < k; r++) m = fmaxf(m, fabsf(T[(size_t)r * ldt + c]));
-    atomic_max_nonneg(&amax[c >> 9], m);
+    for (int seg = 0; 512 * seg < k; seg++) {
+        float m = 0.0f;
+        const int r1 = min(k, 512 * (seg + 1));
+        for (int r = 512 * seg; r < r1; r++) m = fmaxf(m, fabsf(T[(size_t)r * ldt + c]));
+        atomic_max_nonneg(&amax[seg * nblk + (c >> 9)], m);
+    }
 }
 
 // scale = amax / 448 (1 for an all-zero block); inv = 1 / scale.
@@ -60,14 +70,14 @@ __global__ void k_scales(const float* __restrict__ amax, float* __restrict__ sca
 
 template <bool FP8>
 __global__ void k_quant_rows(const float* __restrict__ L, int ldl, uint8_t* __restrict__ out, int rows, int k,
-                             const float* __restrict__ inv) {
+                             const float* __restrict__ inv, int nblk) {
     const size_t total = (size_t)rows * k / 4;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
         const size_t e = i * 4;
         const int r = (int)(e / k), c = (int)(e - (size_t)r * k);
         float4 v = *reinterpret_cast<const float4*>(L + (size_t)r * ldl + c);
         if (FP8) {
-            const float s = inv[r >> 9];
+            const float s = inv[(c >> 9) * nblk + (r >> 9)];  // the four columns share a 512-wide K segment
             __nv_fp8x4_e4m3 q(make_float4(v.x * s, v.y * s, v.z * s, v.w * s));
             *reinterpret_cast<__nv_fp8x4_e4m3*>(out + e) = q;
         } else {
@@ -82,7 +92,7 @@ __global__ void k_quant_rows(const float* __restrict__ L, int ldl, uint8_t* __re
 // out[c][r] = q(T[r][c]) for r < k, c < cols: 32 x 32 tiles through shared memory.
 template <bool FP8>
 __global__ void __launch_bounds__(256) k_quant_trans(const float* __restrict__ T, int ldt, uint8_t* __restrict__ out,
-                                                     int k, int cols, const float* __restrict__ inv) {
+                                                     int k, int cols, const float* __restrict__ inv, int nblk) {
     __shared__ float tile[32][33];
     const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
@@ -98,7 +108,7 @@ __global__ void __launch_bounds__(256) k_quant_trans(const float* __restrict__ T
         if (r < k && c < cols) {
             const float v = tile[tx][ty + j];
             if (FP8) {
-                __nv_fp8_e4m3 q(v * inv[c >> 9]);
+                __nv_fp8_e4m3 q(v * inv[(r >> 9) * nblk + (c >> 9)]);
                 out[(size_t)c * k + r] = *reinterpret_cast<uint8_t*>(&q);
             } else {
                 __nv_bfloat16 q = __float2bfloat16_rn(v);
@@ -219,8 +229,9 @@ int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, in
 
 // Rounds the panel of a block step to the tensor-core operand type.
 // L: rows_l x k (ld ldl), T: k x cols_t (ld ldt); aq: rows_l x k, bq:
-// cols_t x k; sc: 3 arrays of nblk floats (absmax, scale, 1/scale) for L,
-// then 3 for T (nblk >= ceil(max(rows_l, cols_t) / 512)).
+// cols_t x k; sc: 3 arrays of kseg(k) * nblk floats (absmax, scale, 1/scale,
+// indexed seg * nblk + block) for L, then 3 for T (nblk >=
+// ceil(max(rows_l, cols_t) / 512)).
 int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
                    uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st) {
     if (rows_l <= 0 || cols_t <= 0) return LP_OK;
@@ -228,24 +239,25 @@ int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l,
     const int qgrid = (int)((q4 + 255) / 256 < 2368 ? (q4 + 255) / 256 : 2368);
     const dim3 tgrid((cols_t + 31) / 32, (k + 31) / 32);
     if (fp8) {
+        const int ns = kseg(k) * nblk;
         float* amax_a = sc;
-        float* scale_a = sc + nblk;
-        float* inv_a = sc + 2 * nblk;
-        float* amax_b = sc + 3 * nblk;
-        float* scale_b = sc + 4 * nblk;
-        float* inv_b = sc + 5 * nblk;
-        LP_CUDA(cudaMemsetAsync(amax_a, 0, sizeof(float) * nblk, st));
-        LP_CUDA(cudaMemsetAsync(amax_b, 0, sizeof(float) * nblk, st));
-        k_absmax_rows<<<rows_l, 128, 0, st>>>(L, ldl, rows_l, k, amax_a);
-        k_absmax_cols<<<(cols_t + 255) / 256, 256, 0, st>>>(T, ldt, k, cols_t, amax_b);
-        k_scales<<<(nblk + 127) / 128, 128, 0, st>>>(amax_a, scale_a, inv_a, nblk);
-        k_scales<<<(nblk + 127) / 128, 128, 0, st>>>(amax_b, scale_b, inv_b, nblk);
-        k_quant_rows<true><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, inv_a);
-        k_quant_trans<true><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, inv_b);
+        float* scale_a = sc + ns;
+        float* inv_a = sc + 2 * ns;
+        float* amax_b = sc + 3 * ns;
+        float* scale_b = sc + 4 * ns;
+        float* inv_b = sc + 5 * ns;
+        LP_CUDA(cudaMemsetAsync(amax_a, 0, sizeof(float) * ns, st));
+        LP_CUDA(cudaMemsetAsync(amax_b, 0, sizeof(float) * ns, st));
+        k_absmax_rows<<<dim3(rows_l, kseg(k)), 128, 0, st>>>(L, ldl, rows_l, k, nblk, amax_a);
+        k_absmax_cols<<<(cols_t + 255) / 256, 256, 0, st>>>(T, ldt, k, cols_t, nblk, amax_b);
+        k_scales<<<(ns + 127) / 128, 128, 0, st>>>(amax_a, scale_a, inv_a, ns);
+        k_scales<<<(ns + 127) / 128, 128, 0, st>>>(amax_b, scale_b, inv_b, ns);
+        k_quant_rows<true><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, inv_a, nblk);
+        k_quant_trans<true><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, inv_b, nblk);
         count_launch(6);
     } else {
-        k_quant_rows<false><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, nullptr);
-        k_quant_trans<false><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, nullptr);
+        k_quant_rows<false><<<qgrid, 256, 0, st>>>(L, ldl, aq, rows_l, k, nullptr, nblk);
+        k_quant_trans<false><<<tgrid, 256, 0, st>>>(T, ldt, bq, k, cols_t, nullptr, nblk);
         count_launch(2);
     }
     LP_CUDA(cudaGetLastError());
@@ -256,9 +268,10 @@ int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l,
 // columns [n_off, n_off+n) of the trailing matrix at c11.
 static int mixed_update(lp_ctx* c, float* c11, int lda, const uint8_t* aq, const uint8_t* bq, int rest, int m_off,
                         int n_off, int m, int n, int kq, bool fp8, const float* sc, int nblk, cudaStream_t st) {
-    const float* scale_a = fp8 ? sc + nblk : nullptr;
-    const float* scale_b = fp8 ? sc + 4 * nblk : nullptr;
-    return launch_umma_update(c11, lda, aq, rest, bq, rest, m_off, n_off, m, n, kq, fp8, scale_a, scale_b,
+    const int ns = kseg(kq) * nblk;
+    const float* scale_a = fp8 ? sc + ns : nullptr;
+    const float* scale_b = fp8 ? sc + 4 * ns : nullptr;
+    return launch_umma_update(c11, lda, aq, rest, bq, rest, m_off, n_off, m, n, kq, fp8, scale_a, scale_b, nblk,
                               static_cast<int*>(c->err.ptr), st);
 }
 
@@ -312,12 +325,12 @@ static int panel_tc(lp_ctx* c, float* dA, int n, int lda, int bs, int K, int nse
     float* l = d + (size_t)bs * lda;
     LP_CHECK(split_panel(winv, bs, t, lda, bs, rest, bs, a_top, b_top, s, nseg));
     LP_CUDA(cudaMemset2DAsync(t, sizeof(float) * (size_t)lda, 0, sizeof(float) * (size_t)rest, bs, s));
-    LP_CHECK(launch_umma_update(t, lda, a_top, bs, b_top, rest, 0, 0, bs, rest, (int)kq, false, nullptr, nullptr,
+    LP_CHECK(launch_umma_update(t, lda, a_top, bs, b_top, rest, 0, 0, bs, rest, (int)kq, false, nullptr, nullptr, 0,
                                 err, s));
     LP_CHECK(prof_end(c, s, LP_STAGE_TOP, e, b * b * r, 8.0 * b * r));
     e = prof_begin(c, s);
     LP_CHECK(split_panel(l, lda, vinv, bs, rest, bs, bs, a_left, b_left, s, nseg));
-    LP_CHECK(launch_umma_update(l, lda, a_left, rest, b_left, bs, 0, 0, rest, bs, (int)kq, false, nullptr, nullptr,
+    LP_CHECK(launch_umma_update(l, lda, a_left, rest, b_left, bs, 0, 0, rest, bs, (int)kq, false, nullptr, nullptr, 0,
                                 err, s));
     return prof_end(c, s, LP_STAGE_LEFT, e, b * b * r, 8.0 * b * r);
 }
@@ -335,7 +348,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
         LP_CHECK(c->dsub.ensure(2 * sizeof(float) * (size_t)128 * bs));
     }
     LP_CHECK(c->q.ensure(4 * esz * pan));
-    LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)nblk));
+    LP_CHECK(c->qs.ensure(2 * 6 * sizeof(float) * (size_t)kseg(bs) * nblk));
     LP_CHECK(c->err.ensure(sizeof(int)));
     // the top / left products: FP32 accuracy (six segments) for the emulated-FP32
     // form.  For BF16 / E4M3 (the panel is rounded to them for the update anyway)
@@ -351,7 +364,7 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
     uint8_t* q = static_cast<uint8_t*>(c->q.ptr);
     uint8_t* aqb[2] = {q, q + 2 * esz * pan};
     uint8_t* bqb[2] = {q + esz * pan, q + 3 * esz * pan};
-    float* scb[2] = {static_cast<float*>(c->qs.ptr), static_cast<float*>(c->qs.ptr) + 6 * nblk};
+    float* scb[2] = {static_cast<float*>(c->qs.ptr), static_cast<float*>(c->qs.ptr) + 6 * (size_t)kseg(bs) * nblk};
     const int nb = n / bs;
     const double b = bs;
 

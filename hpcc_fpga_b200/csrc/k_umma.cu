@@ -1,6 +1,7 @@
 // inner stage on the 5th-generation tensor cores (mixed-precision form):
 //
-//     C(m x n, FP32) += scale_a[m/512] * scale_b[n/512] * (Aq * Bq^T)
+//     C(m x n, FP32) += sum over 512-wide K segments s of
+//                       scale_a[s][m/512] * scale_b[s][n/512] * (Aq_s * Bq_s^T)
 //
 // Aq: the left panel rounded to BF16 (or FP8 E4M3), m x k, k contiguous;
 // Bq: the top panel rounded the same way and stored transposed, n x k.
@@ -42,9 +43,11 @@ constexpr int UEPI = 8;            // epilogue warps
 constexpr int UT = 32 * (2 + UEPI);
 constexpr int kTileBytesA = UM * UKB;
 constexpr int kScratchFloats = 32 * 33;  // per epilogue warp: one 32 x 32 block, padded
-// Ring depth: 4 stages of 32 KB for TN = 128, 3 of 48 KB for TN = 256.
+// Ring depth: as deep as 227 KB of shared memory allows beside the epilogue's
+// transpose scratch (33 KB): 6 stages of 32 KB for TN = 128, 4 of 48 KB for
+// TN = 256.
 template <int TN>
-__host__ __device__ constexpr int stages() { return TN == 128 ? 4 : 3; }
+__host__ __device__ constexpr int stages() { return TN == 128 ? 6 : 4; }
 template <int TN>
 __host__ __device__ constexpr int stage_bytes() { return kTileBytesA + TN * UKB; }
 template <int TN>
@@ -52,6 +55,7 @@ constexpr size_t umma_smem() {
     return (size_t)stages<TN>() * stage_bytes<TN>() + sizeof(float) * UEPI * kScratchFloats + 1024 /*align slack*/ +
            256 /*barriers*/;
 }
+static_assert(umma_smem<128>() <= 232448 && umma_smem<256>() <= 232448, "umma shared memory");
 constexpr uint32_t kSpinLimit = 1u << 26;
 constexpr uint64_t kWaitNs = 500ull * 1000 * 1000;
 
@@ -170,13 +174,21 @@ __host__ __device__ constexpr uint32_t idesc_value() {
            ((uint32_t)(UM >> 4) << 24);
 }
 
-template <bool FP8, int TN>
+// SEG (E4M3 with K longer than 512): one absmax scale per 512 x 512 block of
+// each operand, i.e. per 512-row block and 512-wide K segment of A and per
+// 512-column block and K segment of B (scale_x[seg * sstride + block]).  The
+// MMA warp accumulates each K segment of a tile into its own accumulator
+// (the two TMEM buffers alternate by segment), and the epilogue adds
+// s_A(seg) s_B(seg) * acc(seg) into per-thread sums before it adds the tile
+// into C once.
+template <bool FP8, int TN, bool SEG = false>
 __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ CUtensorMap map_a,
                                                        const __grid_constant__ CUtensorMap map_b,
                                                        float* __restrict__ C, int ldc, int m_off, int n_off,
                                                        int tiles_n, int tiles, int kbytes,
                                                        const float* __restrict__ scale_a,
-                                                       const float* __restrict__ scale_b, int* __restrict__ err) {
+                                                       const float* __restrict__ scale_b, int nseg, int sstride,
+                                                       int* __restrict__ err) {
     constexpr int USTAGES = stages<TN>();
     constexpr int kStageBytes = stage_bytes<TN>();
     constexpr int kBlk = TN / 64;  // 32-column blocks per epilogue warp
@@ -249,7 +261,44 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
             }
         }
     } else if (warp == 1) {
-        if (lane == 0) {  // MMA issuer
+        if (lane == 0 && SEG) {  // MMA issuer, one accumulator per 512-wide K segment
+            constexpr uint32_t idesc = idesc_value<FP8, TN>();
+            const int ks = KT / nseg;  // ring stages per segment
+            int it = 0, u = 0;
+            bool ok = true;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                for (int seg = 0; seg < nseg && ok; seg++, u++) {
+                    const int b = u & 1;
+                    if (!mbar_wait(&acc_empty[b], ((u >> 1) & 1) ^ 1, abort_flag)) {
+                        atomicExch(err, kErrEmptyWait);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t acc = tmem + (uint32_t)(b * TN);
+                    for (int kk = 0; kk < ks; kk++, it++) {
+                        const int s = it % USTAGES;
+                        if (!mbar_wait(&full[s], (it / USTAGES) & 1, abort_flag)) {
+                            atomicExch(err, kErrFullWait);
+                            *abort_flag = 1;
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sa = smem_u32(ring + s * kStageBytes);
+                        const uint32_t sb = sa + kTileBytesA;
+#pragma unroll
+                        for (int j = 0; j < kSteps; j++)
+                            umma<FP8>(acc, desc_sw128(sa + 32 * j), desc_sw128(sb + 32 * j), idesc,
+                                      (kk | j) ? 1u : 0u);
+                        umma_commit(&empty[s]);
+                    }
+                    if (ok) umma_commit(&acc_full[b]);
+                }
+            }
+            umma_commit(done);  // tracks every MMA issued above, also on the abort path
+        } else if (lane == 0) {  // MMA issuer
             constexpr uint32_t idesc = idesc_value<FP8, TN>();
             int it = 0, i = 0;
             bool ok = true;
@@ -281,6 +330,61 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
                 if (ok) umma_commit(&acc_full[b]);
             }
             umma_commit(done);  // tracks every MMA issued above, also on the abort path
+        }
+    } else if (SEG) {  // epilogue, per-segment scales
+        const int ew = warp - 2;
+        const int quarter = warp & 3;      // TMEM lanes this warp may read
+        const int half = ew >> 2;          // columns [TN/2 half, TN/2 half + TN/2)
+        float* scr = scratch + ew * kScratchFloats;
+        int u = 0;
+        bool okw = true;
+        for (int t = blockIdx.x; t < tiles && okw; t += gridDim.x) {
+            int m0, n0;
+            tile_origin(t, tiles_n, tiles, m_off, n_off, TN, &m0, &n0);
+            const int r0 = m0 + quarter * 32, c0 = n0 + half * (TN / 2);
+            float sum[kBlk][32];  // lane = tile row, 32 consecutive columns per block
+#pragma unroll
+            for (int blk = 0; blk < kBlk; blk++)
+#pragma unroll
+                for (int c = 0; c < 32; c++) sum[blk][c] = 0.0f;
+            for (int seg = 0; seg < nseg; seg++, u++) {
+                const int b = u & 1;
+                // one decision per warp: tcgen05.ld below is warp-collective
+                const bool got = mbar_wait(&acc_full[b], (u >> 1) & 1, abort_flag);
+                if (!__all_sync(0xffffffffu, got)) {
+                    if (lane == 0) atomicExch(err, kErrDoneWait);
+                    *abort_flag = 1;
+                    okw = false;
+                    break;
+                }
+                tc_fence_after();
+                const float sc = scale_a[seg * sstride + (m0 >> 9)] * scale_b[seg * sstride + (n0 >> 9)];
+                const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * TN + half * (TN / 2));
+#pragma unroll
+                for (int blk = 0; blk < kBlk; blk++) {
+                    uint32_t a[32];
+                    tmem_ld32(taddr + 32 * blk, a);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < 32; c++) sum[blk][c] = fmaf(sc, __uint_as_float(a[c]), sum[blk][c]);
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&acc_empty[b]);
+            }
+            if (!okw) break;
+#pragma unroll
+            for (int blk = 0; blk < kBlk; blk++) {
+#pragma unroll
+                for (int c = 0; c < 32; c++) scr[lane * 33 + c] = sum[blk][c];
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < 32; r++) {
+                    float* dst = C + (size_t)(r0 + r) * ldc + c0 + 32 * blk + lane;
+                    *dst = *dst + scr[r * 33 + lane];
+                }
+                __syncwarp();
+            }
         }
     } else {  // epilogue
         const int ew = warp - 2;
@@ -406,6 +510,8 @@ int umma_init_attrs() {
                                  (int)umma_smem<256>()));
     LP_CUDA(cudaFuncSetAttribute(k_umma_update<true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)umma_smem<256>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_update<true, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<128>()));
     return LP_OK;
 }
 
@@ -413,17 +519,24 @@ int umma_init_attrs() {
 // product of aq (rows x k, k contiguous) and bq (cols x k).  aq_rows/bq_rows
 // are the operands' full row counts (the tensor-map extents); m, n, m_off,
 // n_off must be multiples of 128; k a multiple of 64 (BF16) / 128 (E4M3).
+// E4M3 scales: scale_a[seg * sstride + m / 512], scale_b[seg * sstride +
+// n / 512] for the 512-wide K segments seg (one segment when k <= 512; k a
+// multiple of 512 above that).
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
-                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
-                       cudaStream_t st) {
+                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b,
+                       int sstride, int* err, cudaStream_t st) {
     if (m <= 0 || n <= 0) return LP_OK;
     const int kbytes = k * (fp8 ? 1 : 2);
     if (m % UM || n % UN || m_off % UM || n_off % UN || kbytes % UKB || ldc % 4 || !aligned16(c) || !aligned16(aq) ||
         !aligned16(bq) || m_off + m > aq_rows || n_off + n > bq_rows)
         return fail(LP_E_INVALID, "umma_update: tile-aligned sizes and 16-byte aligned operands required");
     if (fp8 && (scale_a == nullptr || scale_b == nullptr)) return fail(LP_E_INVALID, "umma_update: fp8 needs scales");
-    // the wide tile where the column range is a multiple of it
-    const bool wide = n % (2 * UN) == 0 && n_off % (2 * UN) == 0;
+    const bool seg = fp8 && k > 512;
+    if (seg && k % 512 != 0) return fail(LP_E_INVALID, "umma_update: E4M3 with k > 512 needs k % 512 == 0");
+    const int nseg = seg ? k / 512 : 1;
+    // the wide tile where the column range is a multiple of it (the segmented E4M3 form keeps its
+    // per-segment sums in registers: narrow tiles only)
+    const bool wide = !seg && n % (2 * UN) == 0 && n_off % (2 * UN) == 0;
     const int tn = wide ? 2 * UN : UN;
     CUtensorMap ma, mb;
     LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8, UM));
@@ -439,18 +552,21 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     constexpr int kPanelSMs = 8;
     const int usable = sms - kPanelSMs > 1 ? sms - kPanelSMs : 1;
     const int grid = tiles < usable ? tiles : usable;
-    if (fp8 && wide)
+    if (seg)
+        k_umma_update<true, 128, true><<<grid, UT, umma_smem<128>(), st>>>(
+            ma, mb, c, ldc, m_off, n_off, tiles_n, tiles, kbytes, scale_a, scale_b, nseg, sstride, err);
+    else if (fp8 && wide)
         k_umma_update<true, 256><<<grid, UT, umma_smem<256>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
-                                                                     kbytes, scale_a, scale_b, err);
+                                                                     kbytes, scale_a, scale_b, 1, sstride, err);
     else if (fp8)
         k_umma_update<true, 128><<<grid, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
-                                                                     kbytes, scale_a, scale_b, err);
+                                                                     kbytes, scale_a, scale_b, 1, sstride, err);
     else if (wide)
         k_umma_update<false, 256><<<grid, UT, umma_smem<256>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
-                                                                      kbytes, nullptr, nullptr, err);
+                                                                      kbytes, nullptr, nullptr, 1, 0, err);
     else
         k_umma_update<false, 128><<<grid, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n, tiles,
-                                                                      kbytes, nullptr, nullptr, err);
+                                                                      kbytes, nullptr, nullptr, 1, 0, err);
     count_launch();
     LP_CUDA(cudaGetLastError());
     return LP_OK;

@@ -758,7 +758,7 @@ int lp_inner_update_tc_dev(lp_ctx* c, int precision, float* dC, int ldc, const f
     const size_t esz = fp8 ? 1 : 2;
     const int nblk = ((m > n ? m : n) + 511) / 512;
     LP_CHECK(c->q.ensure(esz * (size_t)bs * ((size_t)m + n)));
-    LP_CHECK(c->qs.ensure(6 * sizeof(float) * (size_t)nblk));
+    LP_CHECK(c->qs.ensure(6 * sizeof(float) * (size_t)kseg(bs) * nblk));
     LP_CHECK(c->err.ensure(sizeof(int)));
     uint8_t* aq = static_cast<uint8_t*>(c->q.ptr);
     uint8_t* bq = aq + esz * (size_t)bs * m;
@@ -766,8 +766,9 @@ int lp_inner_update_tc_dev(lp_ctx* c, int precision, float* dC, int ldc, const f
     cudaStream_t st = c->stream;
     LP_CUDA(cudaMemsetAsync(c->err.ptr, 0, sizeof(int), st));
     LP_CHECK(quantize_panel(dL, ldl, dT, ldt, m, n, bs, fp8, aq, bq, sc, nblk, st));
-    LP_CHECK(launch_umma_update(dC, ldc, aq, m, bq, n, 0, 0, m, n, bs, fp8, fp8 ? sc + nblk : nullptr,
-                                fp8 ? sc + 4 * nblk : nullptr, static_cast<int*>(c->err.ptr), st));
+    const size_t ns = (size_t)kseg(bs) * nblk;
+    LP_CHECK(launch_umma_update(dC, ldc, aq, m, bq, n, 0, 0, m, n, bs, fp8, fp8 ? sc + ns : nullptr,
+                                fp8 ? sc + 4 * ns : nullptr, nblk, static_cast<int*>(c->err.ptr), st));
     int herr = 0;
     LP_CUDA(cudaMemcpyAsync(&herr, c->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
     LP_CUDA(cudaStreamSynchronize(st));

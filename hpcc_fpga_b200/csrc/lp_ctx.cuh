@@ -37,8 +37,11 @@ int gefa_mixed(lp_ctx* c, int precision, float* dA, int n, int lda, int bs, cuda
 // Panel work of block step K (lu, top, left; Lt into lt), on stream st; the
 // left stage covers the rows below the diagonal block up to row_end (-1: n).
 int panel_f32(lp_ctx* c, float* dA, int n, int lda, int bs, int K, float* lt, cudaStream_t st, int row_end = -1);
+// E4M3: one absmax scale per 512 x 512 block (512 rows of L / columns of T by
+// a 512-wide K segment); sc holds 6 arrays of kseg(k) * nblk floats.
 int quantize_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, bool fp8,
                    uint8_t* aq, uint8_t* bq, float* sc, int nblk, cudaStream_t st);
+inline int kseg(int k) { return (k + 511) / 512; }
 // Split-BF16 operands (exact three-term split; 6 or 3 K-segments) of a block step.
 int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
                 uint8_t* bq, cudaStream_t st, int nseg = 6);
@@ -47,9 +50,11 @@ int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, in
 int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st);
 int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st);
 int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, cudaStream_t st);
+// E4M3 scales: scale_x[seg * sstride + block] per 512-wide K segment and
+// 512-row (A) / 512-column (B) block (k_umma.cu).
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
-                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b, int* err,
-                       cudaStream_t st);
+                       int n_off, int m, int n, int k, bool fp8, const float* scale_a, const float* scale_b,
+                       int sstride, int* err, cudaStream_t st);
 int umma_init_attrs();
 int batch_init_attrs();
 int validate_batch(int count, const lp_system* systems);
@@ -58,6 +63,14 @@ int validate_batch(int count, const lp_system* systems);
 // into dA / dB; nrhs may then carry the solve-only flag (factors present).
 int launch_batch(lp_ctx* c, const lp_system* d_sorted, int count, float* dA, float* dB, const lp_batch_config& cfg,
                  int* d_next, cudaStream_t st, bool absolute = false);
+// The refined form: factor (trailing updates in BF16 on the tensor cores if
+// bf16), solve and FP64 refinement of every system in one persistent launch.
+// dA0: the original matrices (same offsets as dA); dB32: FP32 work vectors,
+// dB64 / dX: FP64 right-hand sides / solutions (offsets b_off); d_iters /
+// d_resid: per descriptor position.
+int launch_batch_ir(lp_ctx* c, bool bf16, const lp_system* d_sorted, int count, float* dA, const float* dA0,
+                    float* dB32, const double* dB64, double* dX, const lp_batch_config& cfg, int max_iters,
+                    int* d_iters, double* d_resid, int* d_next, cudaStream_t st);
 constexpr int kBatchSolveOnly = 1 << 8;
 // x = LU \ b, then FP64 refinement against the original matrix a0 until the
 // HPL scaled residual is <= 16 or max_iters refinements were made.
@@ -147,6 +160,11 @@ struct lp_ctx {
     lp::Workspace psync, pat, pdesc, pw, pipvt;  // pivoting: barrier + exchange area, transposed U12,
                                                  // interchange permutations, solve vectors, ipvt
     lp::Workspace bsys, bnext;                // batched: sorted system descriptors, work counter
+    lp::Workspace bA0, bB32, bout, bsys_ir;   // refined batch: original matrices, FP32 vectors, per-system results,
+                                              // sorted descriptors
+    lp::Workspace hA, hB, hX;                 // host-buffer batch: device copies of A, B64, X64
+    uint64_t bir_hash = 0;                    // descriptors + configuration of the cached refined graph
+    cudaGraphExec_t bgraph_ir = nullptr;      // refined batched launch, captured once, replayed
     lp::Workspace tA, tB;                     // batched autotuner: scratch copies of the inputs
     uint64_t bsys_hash = 0;                   // descriptors + configuration of the cached graph
     cudaGraphExec_t bgraph = nullptr;         // batched launch, captured once, replayed
@@ -163,10 +181,12 @@ struct lp_ctx {
     long long prof_calls[LP_NSTAGES] = {0};
     void release_all() {
         lp::Workspace* all[] = {&lt, &dsub, &lti, &q, &qs, &err, &tri, &tq, &gw, &gerr, &dA, &dA0, &dB, &dB64, &dX, &dR, &dCol,
-                                &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB};
+                                &dnorm, &gmw, &f64a, &f64b, &f64lt, &f64w, &psync, &pat, &pdesc, &pw, &pipvt, &bsys, &bnext, &tA, &tB, &bA0, &bB32, &bout, &bsys_ir, &hA, &hB, &hX};
         for (auto* w : all) w->release();
         if (bgraph != nullptr) cudaGraphExecDestroy(bgraph);
         bgraph = nullptr;
+        if (bgraph_ir != nullptr) cudaGraphExecDestroy(bgraph_ir);
+        bgraph_ir = nullptr;
         for (auto e : prof_ev) cudaEventDestroy(e);
         prof_ev.clear();
         if (prof_base != nullptr) cudaEventDestroy(prof_base);

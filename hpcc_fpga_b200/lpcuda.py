@@ -185,6 +185,10 @@ def lib() -> ctypes.CDLL:
     L.lp_batch_solve_dev.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig),
                                      ctypes.POINTER(LpBatchStats)]
     L.lp_batch_autotune.argtypes = [_VP, _I, ctypes.POINTER(LpSystem), _VP, _VP, ctypes.POINTER(LpBatchConfig)]
+    L.lp_batch_solve_ir_dev.argtypes = [_VP, _I, _I, ctypes.POINTER(LpSystem), _VP, _VP, _VP, _I,
+                                        ctypes.POINTER(LpBatchConfig), ctypes.POINTER(LpBatchStats), _VP, _VP]
+    L.lp_batch_solve.argtypes = [_VP, _I, _I, ctypes.POINTER(LpSystem), _F32P, _F64P, _F64P, _I,
+                                 ctypes.POINTER(LpBatchConfig), ctypes.POINTER(LpBatchStats), _VP, _VP]
     L.lp_generate_reference.argtypes = [_F32P, _F32P, _I, _I, ctypes.POINTER(ctypes.c_float),
                                         ctypes.POINTER(ctypes.c_float)]
     L.lp_generate_baseline.argtypes = [_F32P, _VP, _VP, _I, ctypes.c_uint, ctypes.c_double]
@@ -397,6 +401,32 @@ class Context:
                                        ctypes.byref(cfg) if cfg is not None else None, ctypes.byref(st)),
               "lp_batch_solve_dev")
         return st.as_dict()
+
+    def batch_solve_ir(self, systems, dA: int, dB64: int, dX: int, precision: str = "bf16", max_iters: int = 10,
+                       cfg: "LpBatchConfig | None" = None):
+        """Refined batch on device buffers: (stats dict, ir_iters array, hpl_resid array)."""
+        arr = (LpSystem * len(systems))(*systems)
+        st = LpBatchStats()
+        its = np.zeros(len(systems), np.int32)
+        res = np.zeros(len(systems), np.float64)
+        check(lib().lp_batch_solve_ir_dev(self._h, PRECISIONS[precision], len(systems), arr, dA, dB64, dX, max_iters,
+                                          ctypes.byref(cfg) if cfg is not None else None, ctypes.byref(st),
+                                          its.ctypes.data, res.ctypes.data), "lp_batch_solve_ir_dev")
+        return st.as_dict(), its, res
+
+    def batch_solve_host(self, systems, A: np.ndarray, B: np.ndarray, precision: str = "bf16", max_iters: int = 10,
+                         cfg: "LpBatchConfig | None" = None):
+        """Refined batch on host buffers: A (float32, factored in place), B (float64
+        right-hand sides) -> (X float64, stats dict, ir_iters, hpl_resid)."""
+        arr = (LpSystem * len(systems))(*systems)
+        st = LpBatchStats()
+        X = np.zeros_like(B)
+        its = np.zeros(len(systems), np.int32)
+        res = np.zeros(len(systems), np.float64)
+        check(lib().lp_batch_solve(self._h, PRECISIONS[precision], len(systems), arr, A, B, X, max_iters,
+                                   ctypes.byref(cfg) if cfg is not None else None, ctypes.byref(st), its.ctypes.data,
+                                   res.ctypes.data), "lp_batch_solve")
+        return X, st.as_dict(), its, res
 
     def batch_autotune(self, systems, dA: int, dB: int) -> LpBatchConfig:
         arr = (LpSystem * len(systems))(*systems)

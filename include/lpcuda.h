@@ -356,6 +356,33 @@ int lp_batch_default_config(lp_batch_config* cfg);
  * context, else the default. */
 int lp_batch_solve_dev(lp_ctx* ctx, int count, const lp_system* systems, float* dA, float* dB,
                        const lp_batch_config* cfg, lp_batch_stats* stats);
+/* The refined batch (no counterpart in the reference): every system of the
+ * batch factored in `precision` — LP_F32: FP32 throughout; LP_BF16_IR: the
+ * trailing updates of systems above small_n_max on the tensor cores with
+ * operands rounded to BF16 and FP32 accumulation (warp-level MMA inside each
+ * system's CTA), the diagonal blocks, the triangular stages and systems
+ * solved whole in shared memory in FP32 — then solved in FP32 and refined in
+ * FP64 against its original matrix (r = b - M x with M widened exactly,
+ * d = LU \ r, x += d) until its HPL scaled residual (eps = DBL_EPSILON/2,
+ * LINPACK/src/host/gmres.c:182-193) is <= 16 or max_iters refinements were
+ * made (0: none).  Factorization, solve and refinement of every system run in
+ * ONE persistent launch (with a device copy of the originals), captured in a
+ * CUDA graph and replayed for the same batch when cfg->use_graph.
+ * dA: the matrices as for lp_batch_solve_dev, overwritten by the factors;
+ * dB64: FP64 right-hand sides (nrhs rows of ldb doubles at b_off); dX: the
+ * FP64 solutions in the same layout.  ir_iters / hpl_resid (optional, host,
+ * count entries, in the caller's order): refinements made and the final
+ * scaled residual per system.  LP_E_NUMERIC if a solution is not finite. */
+int lp_batch_solve_ir_dev(lp_ctx* ctx, int precision, int count, const lp_system* systems, float* dA,
+                          const double* dB64, double* dX, int max_iters, const lp_batch_config* cfg,
+                          lp_batch_stats* stats, int* ir_iters, double* hpl_resid);
+/* The same over host buffers (the batch analogue of lp_solve_host): A (host,
+ * packed as for the device call) is copied in, factored and written back with
+ * the factors; B (host, FP64 right-hand sides) in, X (host, FP64 solutions)
+ * out.  stats->seconds is the device time of the launch alone. */
+int lp_batch_solve(lp_ctx* ctx, int precision, int count, const lp_system* systems, float* A, const double* B,
+                   double* X, int max_iters, const lp_batch_config* cfg, lp_batch_stats* stats, int* ir_iters,
+                   double* hpl_resid);
 /* Times candidate configurations per size bucket on copies of the batch
  * (dA, dB are not modified) and returns the fastest in out; the result also
  * becomes the context's default for lp_batch_solve_dev(cfg = NULL). */

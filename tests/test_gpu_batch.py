@@ -143,3 +143,104 @@ def test_batch_rejects_bad_systems(ctx, lp):
     assert e.value.status == lp.LP_E_INVALID
     with pytest.raises(lp.LpError):
         ctx.batch_solve([lp.LpSystem(8, 17, 8, 8, 0, 0)], 1 << 20, 1 << 20)
+
+
+def _refined_batch(lp, sizes, nrhs, seed=3):
+    """A batch of seeded diagonally dominant systems whose FP64 right-hand
+    sides have exact solutions: x_q = (q + 1) * ones."""
+    b = hb.Batch(sizes, nrhs)
+    B64 = np.zeros(b.B.shape, np.float64)
+    for i, s in enumerate(b.systems):
+        A, b64, _ = lp.generate_baseline(s.n, seed + i, 1.0)
+        b.mat(i)[:, :] = A
+        for q in range(s.nrhs):
+            B64[s.b_off + q * s.ldb:s.b_off + q * s.ldb + s.n] = (q + 1) * b64
+    return b, B64
+
+
+def _x_of(b, X, i):
+    s = b.systems[i]
+    return X[s.b_off:s.b_off + s.nrhs * s.ldb].reshape(s.nrhs, s.ldb)[:, :s.n]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["f32", "bf16"])
+def test_batch_refined_reaches_hpl_threshold(ctx, dev, lp, prec):
+    """Every system of a mixed batch (whole-in-shared-memory and blocked
+    sizes, 1..16 right-hand sides) refines in FP64 to the HPL threshold
+    (gmres.c:182-193) inside the one launch, and the FP64-oracle error (the
+    exact solutions are (q + 1) * ones) is far below FP32 accuracy."""
+    sizes = [1, 7, 32, 100, 128, 129, 200, 256, 300, 513, 777, 1024]
+    nrhs = [1, 2, 16, 3, 1, 5, 8, 1, 4, 2, 16, 3]
+    b, B64 = _refined_batch(lp, sizes, nrhs)
+    dA, dB = dev.put(b.A), dev.put(B64)
+    dX = dev.empty(B64.shape, np.float64)
+    st, its, res = ctx.batch_solve_ir(b.systems, dA.data_ptr(), dB.data_ptr(), dX.data_ptr(), prec, max_iters=10)
+    X = dev.get(dX)
+    assert st["systems"] == len(sizes)
+    for i, s in enumerate(b.systems):
+        x = _x_of(b, X, i)
+        want = np.arange(1, s.nrhs + 1, dtype=np.float64)[:, None]
+        err = np.abs(x - want).max() / want.max()
+        assert res[i] <= 16.0, f"system {i} (n={s.n}): hpl {res[i]}"
+        assert its[i] <= 5, f"system {i} (n={s.n}): {its[i]} refinements"
+        assert err < 1e-10, f"system {i} (n={s.n}): err {err}"
+
+
+@pytest.mark.gpu
+def test_batch_bf16_factors_are_the_tensor_core_form(ctx, dev, lp):
+    """The BF16 form's factors of a blocked-path system differ from the FP32
+    form's by the BF16 rounding of the trailing updates (not more, not zero),
+    while systems solved whole in shared memory are factored in FP32 by both."""
+    sizes, nrhs = [64, 512], [1, 1]
+    b, B64 = _refined_batch(lp, sizes, nrhs, seed=9)
+    out = {}
+    for prec in ("f32", "bf16"):
+        dA, dB = dev.put(b.A), dev.put(B64)
+        dX = dev.empty(B64.shape, np.float64)
+        ctx.batch_solve_ir(b.systems, dA.data_ptr(), dB.data_ptr(), dX.data_ptr(), prec, max_iters=0)
+        out[prec] = dev.get(dA)
+    s0, s1 = b.systems
+    small = slice(s0.a_off, s0.a_off + s0.n * s0.lda)
+    big = slice(s1.a_off, s1.a_off + s1.n * s1.lda)
+    assert np.array_equal(out["f32"][small], out["bf16"][small])
+    d = np.abs(out["f32"][big] - out["bf16"][big]).max() / np.abs(out["f32"][big]).max()
+    assert 0.0 < d < 2e-3, d
+
+
+@pytest.mark.gpu
+def test_batch_host_buffers_match_device_call_and_replay(ctx, dev, lp):
+    """lp_batch_solve (host buffers) returns exactly what the device entry
+    point returns, and the second device call replays the captured graph with
+    identical results."""
+    sizes, nrhs = [50, 130, 400, 900], [2, 1, 3, 8]
+    b, B64 = _refined_batch(lp, sizes, nrhs, seed=21)
+    A_host = b.A.copy()
+    X_host, st_h, its_h, res_h = ctx.batch_solve_host(b.systems, A_host, B64, "bf16", max_iters=10)
+    runs = []
+    dA, dB = dev.put(b.A), dev.put(B64)
+    dX = dev.empty(B64.shape, np.float64)
+    for _ in range(2):  # the same buffers both times: the second call replays the graph
+        dA.copy_(dev.torch.from_numpy(b.A).cuda())
+        dX.zero_()
+        dev.torch.cuda.synchronize()
+        st, its, res = ctx.batch_solve_ir(b.systems, dA.data_ptr(), dB.data_ptr(), dX.data_ptr(), "bf16",
+                                          max_iters=10)
+        runs.append((dev.get(dA), dev.get(dX), st, its, res))
+    assert np.array_equal(runs[0][1], runs[1][1]) and np.array_equal(runs[0][0], runs[1][0])
+    assert runs[1][2]["graph_replayed"] == 1
+    assert np.array_equal(X_host, runs[0][1]) and np.array_equal(A_host, runs[0][0])
+    assert np.array_equal(its_h, runs[0][3]) and np.array_equal(res_h, runs[0][4])
+
+
+@pytest.mark.gpu
+def test_batch_refined_rejects_bad_arguments(ctx, dev, lp):
+    b, B64 = _refined_batch(lp, [40], [1])
+    dA, dB = dev.put(b.A), dev.put(B64)
+    dX = dev.empty(B64.shape, np.float64)
+    with pytest.raises(lp.LpError) as e:
+        ctx.batch_solve_ir(b.systems, dA.data_ptr(), dB.data_ptr(), dX.data_ptr(), "fp8")
+    assert e.value.status == lp.LP_E_INVALID
+    with pytest.raises(lp.LpError) as e:
+        ctx.batch_solve_ir(b.systems, dA.data_ptr(), dB.data_ptr(), dX.data_ptr(), "bf16", max_iters=-1)
+    assert e.value.status == lp.LP_E_INVALID

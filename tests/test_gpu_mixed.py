@@ -69,6 +69,45 @@ def test_inner_update_tc_fp8(ctx, dev, m, n, bs):
     assert np.all(np.abs(got - exact) <= bound)
 
 
+def q_fp8_blocks(torch, L):
+    """Per 512 x 512 block (512 rows by a 512-wide K segment): s = amax/448,
+    q = e4m3(L * (1/s)) dequantized — the E4M3 operand of a K > 512 update."""
+    out = np.empty(L.shape, np.float64)
+    for k0 in range(0, L.shape[1], 512):
+        out[:, k0:k0 + 512] = q_fp8_rows(torch, np.ascontiguousarray(L[:, k0:k0 + 512]))
+    return out
+
+
+@pytest.mark.parametrize("m,n,bs", [(512, 384, 1024), (640, 512, 2048)])
+def test_inner_update_tc_fp8_per_512_block_scales(ctx, dev, m, n, bs):
+    """With K > 512 every 512 x 512 block of each operand carries its own
+    absmax scale.  K segment s of L is scaled by 1e-6^s and of T by 1e6^s, so
+    every segment contributes alike to L T: one scale per 512 x K block of L
+    would flush the small segments to E4M3 zero (their values fall below the
+    format's smallest subnormal), per-block scales keep them at full E4M3
+    precision.  Checked against the per-block rounding emulated in FP64 within
+    the FP32 accumulation bound; the one-scale-per-512-x-K emulation misses
+    that bound (so the test tells the two apart)."""
+    rng = np.random.default_rng(5 * m + n + bs)
+    nseg = bs // 512
+    sl = np.repeat(np.float32(1e-6) ** np.arange(nseg, dtype=np.float32), 512)
+    st = np.repeat(np.float32(1e6) ** np.arange(nseg, dtype=np.float32), 512)
+    C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
+    L = (rng.uniform(-1, 1, (m, bs)).astype(np.float32) * sl[None, :]).astype(np.float32)
+    T = (rng.uniform(-1, 1, (bs, n)).astype(np.float32) * np.float32(0.01) * st[:, None]).astype(np.float32)
+    dC, dL, dT = dev.put(C), dev.put(L), dev.put(T)
+    ctx.inner_update_tc("fp8", dC.data_ptr(), n, dL.data_ptr(), bs, dT.data_ptr(), n, m, n, bs)
+    got = dev.get(dC).astype(np.float64)
+    Lq = q_fp8_blocks(dev.torch, L)
+    Tq = q_fp8_blocks(dev.torch, np.ascontiguousarray(T.T)).T
+    exact = C.astype(np.float64) + Lq @ Tq
+    bound = (bs + 4) * FLT_EPS * (np.abs(C) + np.abs(Lq) @ np.abs(Tq))
+    assert np.all(np.abs(got - exact) <= bound)
+    Lo = q_fp8_rows(dev.torch, L)
+    To = q_fp8_rows(dev.torch, np.ascontiguousarray(T.T)).T
+    assert np.any(np.abs(C.astype(np.float64) + Lo @ To - exact) > bound)
+
+
 def test_gefa_prec_f32_is_gefa(ctx, dev):
     n, bs = 1024, 256
     A, _, _, _ = oracle.gen_reference(n)
