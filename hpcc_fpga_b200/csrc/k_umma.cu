@@ -179,8 +179,8 @@ __host__ __device__ constexpr uint32_t idesc_value() {
 // 512-column block and K segment of B (scale_x[seg * sstride + block]).  The
 // MMA warp accumulates each K segment of a tile into its own accumulator
 // (the two TMEM buffers alternate by segment), and the epilogue adds
-// s_A(seg) s_B(seg) * acc(seg) into per-thread sums before it adds the tile
-// into C once.
+// s_A(seg) s_B(seg) * acc(seg) into per-thread sums that start from the tile
+// of C, then writes the tile back once.
 template <bool FP8, int TN, bool SEG = false>
 __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ CUtensorMap map_a,
                                                        const __grid_constant__ CUtensorMap map_b,
@@ -342,11 +342,22 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
             int m0, n0;
             tile_origin(t, tiles_n, tiles, m_off, n_off, TN, &m0, &n0);
             const int r0 = m0 + quarter * 32, c0 = n0 + half * (TN / 2);
-            float sum[kBlk][32];  // lane = tile row, 32 consecutive columns per block
+            // sums in the accumulator layout (lane = tile row, 32 consecutive columns per block),
+            // started from this warp's 32 x TN/2 piece of C: coalesced row loads, transposed
+            // through shared memory while the first segment's products run
+            float sum[kBlk][32];
 #pragma unroll
-            for (int blk = 0; blk < kBlk; blk++)
+            for (int blk = 0; blk < kBlk; blk++) {
+                float cv[32];
 #pragma unroll
-                for (int c = 0; c < 32; c++) sum[blk][c] = 0.0f;
+                for (int r = 0; r < 32; r++) cv[r] = C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane];
+#pragma unroll
+                for (int r = 0; r < 32; r++) scr[r * 33 + lane] = cv[r];
+                __syncwarp();
+#pragma unroll
+                for (int c = 0; c < 32; c++) sum[blk][c] = scr[lane * 33 + c];
+                __syncwarp();
+            }
             for (int seg = 0; seg < nseg; seg++, u++) {
                 const int b = u & 1;
                 // one decision per warp: tcgen05.ld below is warp-collective
@@ -379,10 +390,7 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
                 for (int c = 0; c < 32; c++) scr[lane * 33 + c] = sum[blk][c];
                 __syncwarp();
 #pragma unroll
-                for (int r = 0; r < 32; r++) {
-                    float* dst = C + (size_t)(r0 + r) * ldc + c0 + 32 * blk + lane;
-                    *dst = *dst + scr[r * 33 + lane];
-                }
+                for (int r = 0; r < 32; r++) C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane] = scr[r * 33 + lane];
                 __syncwarp();
             }
         }

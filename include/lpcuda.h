@@ -44,7 +44,8 @@ extern "C" {
 /* Factorization precision.  LP_F32: every stage in FP32 (the reference's
  * single-precision build).  LP_BF16_IR / LP_FP8_IR: the trailing (inner)
  * update runs on the tensor cores with operands rounded to BF16 or to FP8
- * E4M3 with one absmax scale per 512x512 block, FP32 accumulation; the
+ * E4M3 with one absmax scale per 512 x 512 block (512 rows of L or columns
+ * of T by a 512-wide K segment), FP32 accumulation; the
  * diagonal-block LU and the triangular updates stay FP32; the solve is
  * refined in FP64 (residual and update) until the HPL scaled residual is
  * at most 16. */
@@ -167,8 +168,9 @@ int lp_inner_update_dev(lp_ctx* ctx, float* dC, int ldc, const float* dLt, int l
                         int m, int n, int bs);
 
 /* inner on the tensor cores: C(m x n) += L(m x bs) * T(bs x n) with L and T
- * rounded to BF16 (LP_BF16_IR) or to E4M3 with one absmax scale per 512-row
- * block of L and 512-column block of T (LP_FP8_IR), FP32 accumulation —
+ * rounded to BF16 (LP_BF16_IR) or to E4M3 with one absmax scale per 512 x 512
+ * block (LP_FP8_IR: per 512 rows of L, or columns of T, by 512-wide K
+ * segment; bs above 512 must be a multiple of 512), FP32 accumulation —
  * the mixed-precision form of inner_update_mm (hpl_torus_PCIE.cl:711-865).
  * L is given row-major (ldl), T row-major (ldt); m, n, bs multiples of 128.
  * Returns LP_E_TIMEOUT if a bounded wait inside the kernel expired. */
