@@ -937,9 +937,10 @@ def main() -> None:
                      "per_unit": "2*m*m*bs flop per trailing update of an m x m trailing matrix",
                      "launches": inner["calls"],
                      # DRAM bytes per trailing update: the n=8192 ncu capture of this kernel
-                     # (profiles/k_sgemm_update_n8192_b512.md) read+wrote 452.4 MB for 503.3 MB of
-                     # algorithmic bytes; scaled by the algorithmic bytes of this run's updates.
-                     "traffic": (inner["bytes"] / inner["calls"] * 452.4 / 503.3) if inner["calls"] else None,
+                     # (profiles/k_sgemm_update_n8192_b512.md) read+wrote 388.6 MB for 440.4 MB of
+                     # algorithmic bytes (a 7168^2 x 512 update); scaled by the algorithmic bytes of
+                     # this run's updates.
+                     "traffic": (inner["bytes"] / inner["calls"] * 388.6 / 440.4) if inner["calls"] else None,
                      "traffic_unit": "bytes per trailing update (scaled from the n=8192 capture)"},
         "stages": {k: {"s": prof[k]["s"], "share": stage_share[k], "calls": prof[k]["calls"]} for k in lp.STAGES
                    if prof[k]["calls"]},
