@@ -49,40 +49,68 @@ namespace {
 using namespace gesl;
 
 constexpr int ICH = 32;        // chunk of the inverse recurrences
-constexpr int IST = 64;        // strip width of the inverse recurrences
-constexpr int BLK2 = SB * SB;  // floats per operator
 constexpr int RS = 32;         // factor rows per ring stage
 constexpr int SPT = SB / RS;   // stages per source tile
 constexpr int STAGE_FLOATS = RS * SB;
-constexpr int kInvTopScratch = SB * IST + SB * ICH;
-constexpr int kInvLeftScratch = IST * (SB + 1) + ICH * SB;
-constexpr int kInvScratch = kInvTopScratch > kInvLeftScratch ? kInvTopScratch : kInvLeftScratch;
+constexpr int OPL = SB + 1;              // row stride of the forward operator (its rows are recurrence chains)
+constexpr int kOpFloats = SB * OPL;
+constexpr int kScratch = 2 * 32 * SB;     // two chunks of the diagonal block (2 x 32 x 128), later the reductions
 constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;  // a bounded wait gives up after 250 ms
 constexpr unsigned kTagFwd = 1, kTagBwd = 2, kTagNever = 0x7fff0000u;
 
-// Columns [c0, c0 + IST) of X for the diagonal block d (kb valid rows and
-// columns; the rest of the 128 x 128 block is the identity) into op (row
-// stride SB).  All 256 threads; scr: kInvTopScratch floats.
-__device__ void inv_top_strip(const float* __restrict__ d, int lda, int kb, int c0, float* scr, float* op) {
-    float* strip = scr;            // SB x IST
-    float* dch = scr + SB * IST;   // SB x ICH
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < SB * IST; idx += GT) {
-        const int r = idx / IST, c = idx - r * IST;
-        strip[idx] = (r == c0 + c) ? 1.0f : 0.0f;
+__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, int src_bytes) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Rows [r0, r0 + rows) x columns [k0, k0 + cols) of the diagonal block d
+// (cols a multiple of 4; entries outside the kb x kb block read as 0) into
+// buf (row stride cols) by 16-byte asynchronous copies, committed as one group.
+__device__ __forceinline__ void load_block(const float* __restrict__ d, int lda, int kb, int r0, int rows, int k0,
+                                           int cols, float* buf) {
+    const int q4 = cols / 4;
+    for (int idx = threadIdx.x; idx < rows * q4; idx += GT) {
+        const int rr = idx / q4, cc = (idx - rr * q4) * 4;
+        const int r = r0 + rr, c = k0 + cc, rem = kb - c;
+        const int bytes = (r < kb && rem > 0) ? (rem >= 4 ? 16 : 4 * rem) : 0;
+        cp_async16(buf + rr * cols + cc, bytes > 0 ? d + (size_t)r * lda + c : d, bytes);
     }
-    for (int r0 = 0; r0 < SB; r0 += ICH) {
+    cp_commit();
+}
+
+// X = (diag(D_kk)^-1 - L)^-1 for the diagonal block d (kb valid rows and
+// columns; the rest of the 128 x 128 block is the identity) into op (row
+// stride SB): the top recurrence applied to the identity, every column at
+// once (columns are independent).  Per 32-row chunk of D (double-buffered
+// asynchronous copies, the next chunk in flight): one thread per column runs
+// the chunk's 32-step recurrence in registers, then all threads apply the
+// chunk to the rows below it.  scr: 2 x 128 x 32 floats.  Waiting for its
+// copies also completes any copies the calling thread issued before.
+__device__ void inv_top_full(const float* __restrict__ d, int lda, int kb, float* scr, float* op) {
+    const int tid = threadIdx.x;
+    for (int idx = tid; idx < SB * SB; idx += GT) op[idx] = (idx / SB == idx % SB) ? 1.0f : 0.0f;
+    load_block(d, lda, kb, 0, SB, 0, ICH, scr);
+    for (int r0 = 0, ch = 0; r0 < SB; r0 += ICH, ch++) {
         const int nr = SB - r0;
-        for (int idx = tid; idx < nr * ICH; idx += GT) {
-            const int rr = idx / ICH, kk = idx - rr * ICH;
-            const int r = r0 + rr, k = r0 + kk;
-            dch[idx] = (r < kb && k < kb) ? d[(size_t)r * lda + k] : (r == k ? 1.0f : 0.0f);
+        float* dch = scr + (ch & 1) * (SB * ICH);  // rows r0.. of columns [r0, r0 + 32), SB x ICH
+        if (r0 + ICH < SB) {
+            load_block(d, lda, kb, r0 + ICH, nr - ICH, r0 + ICH, ICH, scr + ((ch + 1) & 1) * (SB * ICH));
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
         }
         __syncthreads();
-        if (tid < IST) {
+        if (kb < SB)  // the identity outside the kb x kb block: diagonal entries at and after kb
+            for (int rr = tid; rr < min(nr, ICH); rr += GT)
+                if (r0 + rr >= kb) dch[rr * ICH + rr] = 1.0f;
+        __syncthreads();
+        if (tid < SB) {
             float x[ICH];
 #pragma unroll
-            for (int k = 0; k < ICH; k++) x[k] = strip[(r0 + k) * IST + tid];
+            for (int k = 0; k < ICH; k++) x[k] = op[(r0 + k) * SB + tid];
 #pragma unroll
             for (int k = 0; k < ICH; k++) {
                 const float xk = x[k] * dch[k * ICH + k];
@@ -91,53 +119,54 @@ __device__ void inv_top_strip(const float* __restrict__ d, int lda, int kb, int 
                 for (int j = k + 1; j < ICH; j++) x[j] = fmaf(xk, dch[j * ICH + k], x[j]);
             }
 #pragma unroll
-            for (int k = 0; k < ICH; k++) strip[(r0 + k) * IST + tid] = x[k];
+            for (int k = 0; k < ICH; k++) op[(r0 + k) * SB + tid] = x[k];
         }
         __syncthreads();
         if (nr > ICH) {
-            const int c = tid & (IST - 1), g = tid / IST;
+            const int c = tid & (SB - 1), g = tid >> 7;
             float x[ICH];
 #pragma unroll
-            for (int k = 0; k < ICH; k++) x[k] = strip[(r0 + k) * IST + c];
-            for (int r = r0 + ICH + g; r < SB; r += GT / IST) {
-                float acc = strip[r * IST + c];
+            for (int k = 0; k < ICH; k++) x[k] = op[(r0 + k) * SB + c];
+            // four rows at a time: independent FMA chains interleave
+#pragma unroll 4
+            for (int r = r0 + ICH + g; r < SB; r += GT / SB) {
+                float acc = op[r * SB + c];
                 const float* drow = dch + (r - r0) * ICH;
 #pragma unroll
                 for (int k = 0; k < ICH; k++) acc = fmaf(x[k], drow[k], acc);
-                strip[r * IST + c] = acc;
+                op[r * SB + c] = acc;
             }
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < SB * IST; idx += GT) {
-        const int r = idx / IST, c = idx - r * IST;
-        op[r * SB + c0 + c] = strip[idx];
-    }
-    __syncthreads();
 }
 
-// Rows [r0s, r0s + IST) of Y for the diagonal block d into op (row stride
-// SB).  All 256 threads; scr: kInvLeftScratch floats.
-__device__ void inv_left_strip(const float* __restrict__ d, int lda, int kb, int r0s, float* scr, float* op) {
-    constexpr int SL = SB + 1;
-    float* strip = scr;            // IST x (SB + 1)
-    float* dch = scr + IST * SL;   // ICH x SB
+// Y = (I - U)^-1 for the diagonal block d into op (row stride OPL): the left
+// recurrence applied to the identity, every row at once (rows are
+// independent).  Per 32-column chunk of D (double-buffered asynchronous
+// copies): one thread per row runs the chunk's recurrence in registers, then
+// all threads apply the chunk to the columns after it, one (row, column)
+// element per thread at a time.  scr: 2 x 32 x 128 floats.
+__device__ void inv_left_full(const float* __restrict__ d, int lda, int kb, float* scr, float* op) {
     const int tid = threadIdx.x;
-    for (int idx = tid; idx < IST * SB; idx += GT) {
+    for (int idx = tid; idx < SB * SB; idx += GT) {
         const int rr = idx / SB, c = idx - rr * SB;
-        strip[rr * SL + c] = (r0s + rr == c) ? 1.0f : 0.0f;
+        op[rr * OPL + c] = (rr == c) ? 1.0f : 0.0f;
     }
-    for (int c0 = 0; c0 < SB; c0 += ICH) {
+    load_block(d, lda, kb, 0, ICH, 0, SB, scr);
+    for (int c0 = 0, ch = 0; c0 < SB; c0 += ICH, ch++) {
         const int nc = SB - c0;
-        for (int idx = tid; idx < ICH * nc; idx += GT) {
-            const int kk = idx / nc, cc = idx - kk * nc;
-            const int k = c0 + kk, c = c0 + cc;
-            dch[idx] = (k < kb && c < kb) ? d[(size_t)k * lda + c] : 0.0f;
+        float* dch = scr + (ch & 1) * (ICH * SB);  // rows [c0, c0 + 32) of columns c0.., ICH x nc
+        if (c0 + ICH < SB) {
+            load_block(d, lda, kb, c0 + ICH, ICH, c0 + ICH, nc - ICH, scr + ((ch + 1) & 1) * (ICH * SB));
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
         }
         __syncthreads();
-        if (tid < IST) {
+        if (tid < SB) {
             float x[ICH];
-            float* row = strip + tid * SL + c0;
+            float* row = op + tid * OPL + c0;
 #pragma unroll
             for (int k = 0; k < ICH; k++) x[k] = row[k];
 #pragma unroll
@@ -148,25 +177,19 @@ __device__ void inv_left_strip(const float* __restrict__ d, int lda, int kb, int
             for (int k = 0; k < ICH; k++) row[k] = x[k];
         }
         __syncthreads();
-        for (int ci = ICH + tid; ci < nc; ci += GT) {
-            float dv[ICH];
+        const int rest = nc - ICH;
+        // four elements at a time: independent FMA chains interleave
+#pragma unroll 4
+        for (int idx = tid; idx < rest * SB; idx += GT) {
+            const int rr = idx / rest, ci = ICH + (idx - rr * rest);
+            const float* row = op + rr * OPL + c0;
+            float acc = row[ci];
 #pragma unroll
-            for (int k = 0; k < ICH; k++) dv[k] = dch[k * nc + ci];
-            for (int rr = 0; rr < IST; rr++) {
-                const float* row = strip + rr * SL + c0;
-                float acc = row[ci];
-#pragma unroll
-                for (int k = 0; k < ICH; k++) acc = fmaf(row[k], dv[k], acc);
-                strip[rr * SL + c0 + ci] = acc;
-            }
+            for (int k = 0; k < ICH; k++) acc = fmaf(row[k], dch[k * nc + ci], acc);
+            op[rr * OPL + c0 + ci] = acc;
         }
         __syncthreads();
     }
-    for (int idx = tid; idx < IST * SB; idx += GT) {
-        const int rr = idx / SB, c = idx - rr * SB;
-        op[(r0s + rr) * SB + c] = strip[rr * SL + c];
-    }
-    __syncthreads();
 }
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -183,20 +206,12 @@ __device__ __forceinline__ void st_pair(unsigned long long* p, unsigned tag, flo
     const unsigned long long w = ((unsigned long long)tag << 32) | (unsigned long long)__float_as_uint(v);
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
-__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, int src_bytes) {
-    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Ring depth per right-hand-side width: as deep as shared memory allows
-// (227 KB per CTA) beside the operator, the inverse scratch and the staged
-// values.
+// (227 KB per CTA) beside the operator, the scratch and the staged values.
 template <int NR>
 __host__ __device__ constexpr int stages() {
-    return NR == 1 ? 7 : NR <= 4 ? 6 : 5;
+    return NR <= 4 ? 7 : 6;
 }
 
 // Published values of one source tile, prefetched into registers: thread t
@@ -286,9 +301,9 @@ __global__ void __launch_bounds__(GT, 1)
                  int* __restrict__ err, int stall) {
     constexpr int STG = stages<NR>();
     extern __shared__ __align__(16) float smem[];
-    float* op = smem;                         // 128 x 128 operator of the tile (Y or X)
-    float* scr = op + BLK2;                   // inverse scratch, later the reductions
-    float* ring = scr + kInvScratch;          // STG x 32 x 128 factor rows
+    float* op = smem;                         // 128 x 128 operator of the tile (Y, row stride OPL; or X)
+    float* scr = op + kOpFloats;              // a chunk of the diagonal block, later the reductions
+    float* ring = scr + kScratch;             // STG x 32 x 128 factor rows
     float* ybuf = ring + STG * STAGE_FLOATS;  // 128 x NR published values of one source tile
     float* inb = ybuf + NR * SB;              // NR x 128 input of the tile (b_j or y_j)
     __shared__ int s_tile;
@@ -340,13 +355,10 @@ __global__ void __launch_bounds__(GT, 1)
         }
         const float* d = a + (size_t)c0 * lda + c0;
         auto invert = [&]() {
-            if (FWD) {
-                inv_left_strip(d, lda, kb, 0, scr, op);
-                inv_left_strip(d, lda, kb, IST, scr, op);
-            } else {
-                inv_top_strip(d, lda, kb, 0, scr, op);
-                inv_top_strip(d, lda, kb, IST, scr, op);
-            }
+            if (FWD)
+                inv_left_full(d, lda, kb, scr, op);
+            else
+                inv_top_full(d, lda, kb, scr, op);
         };
         bool inverted = false;
         float p[NR];
@@ -438,7 +450,7 @@ __global__ void __launch_bounds__(GT, 1)
 #pragma unroll 16
             for (int kk = 0; kk < SB / 2; kk++) {
                 const int k = hh * (SB / 2) + kk;
-                const float m = op[k * SB + i];
+                const float m = op[k * (FWD ? OPL : SB) + i];
 #pragma unroll
                 for (int r = 0; r < NR; r++) pr[r] = fmaf(m, acc[r * SB + k], pr[r]);
             }
@@ -461,10 +473,10 @@ __global__ void __launch_bounds__(GT, 1)
 template <int NR>
 constexpr size_t sweep_smem() {
     return sizeof(float) *
-           ((size_t)BLK2 + kInvScratch + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
+           ((size_t)kOpFloats + kScratch + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
 }
-// the reductions fit in the inverse scratch
-static_assert(4 * 16 * SB <= kInvScratch, "reduction buffers exceed the scratch");
+// a chunk of the diagonal block and the reductions fit in the scratch
+static_assert(2 * SB * ICH <= kScratch && 4 * 16 * SB <= kScratch, "scratch");
 static_assert(sweep_smem<1>() <= 227 * 1024 && sweep_smem<4>() <= 227 * 1024 && sweep_smem<16>() <= 227 * 1024,
               "sweep shared memory");
 
