@@ -361,9 +361,12 @@ __global__ void __launch_bounds__(GT, 1)
                 inv_top_full(d, lda, kb, scr, op);
         };
         bool inverted = false;
-        float p[NR];
+        // PS partial sums per right-hand side (rows round-robin) so that one right-hand side's
+        // FMAs form independent chains; combined in a fixed order at the end of the tile
+        constexpr int PS = NR == 1 ? 4 : 1;
+        float p[NR * PS];
 #pragma unroll
-        for (int q = 0; q < NR; q++) p[q] = 0.0f;
+        for (int q = 0; q < NR * PS; q++) p[q] = 0.0f;
         bool ok = *(volatile int*)err == 0;
         ok = __syncthreads_and(ok) != 0;
         Pending<NR> pd;
@@ -391,7 +394,7 @@ __global__ void __launch_bounds__(GT, 1)
                     }
                 } else {
 #pragma unroll
-                    for (int q = 0; q < NR; q++) p[q] = fmaf(y[q], v, p[q]);
+                    for (int q = 0; q < NR; q++) p[q * PS + r % PS] = fmaf(y[q], v, p[q * PS + r % PS]);
                 }
             }
         };
@@ -432,30 +435,39 @@ __global__ void __launch_bounds__(GT, 1)
         float* red = scr;                 // NR x 128: the upper half's sums
         float* acc = red + NR * SB;       // NR x 128
         float* part = acc + NR * SB;      // 2 x NR x 128
+        if constexpr (PS > 1) {
+#pragma unroll
+            for (int q = 0; q < NR; q++) p[q * PS] = (p[q * PS] + p[q * PS + 1]) + (p[q * PS + 2] + p[q * PS + 3]);
+        }
         if (h == 1) {
 #pragma unroll
-            for (int q = 0; q < NR; q++) red[q * SB + c] = p[q];
+            for (int q = 0; q < NR; q++) red[q * SB + c] = p[q * PS];
         }
         ok = __syncthreads_and(ok) != 0;
         if (h == 0) {
 #pragma unroll
-            for (int q = 0; q < NR; q++) acc[q * SB + c] = (q < g && c < kb) ? inb[q * SB + c] + p[q] + red[q * SB + c] : 0.0f;
+            for (int q = 0; q < NR; q++)
+                acc[q * SB + c] = (q < g && c < kb) ? inb[q * SB + c] + p[q * PS] + red[q * SB + c] : 0.0f;
         }
         __syncthreads();
         {
             const int i = tid & (SB - 1), hh = tid >> 7;
-            float pr[NR];
+            float pr[NR * PS];
 #pragma unroll
-            for (int r = 0; r < NR; r++) pr[r] = 0.0f;
+            for (int r = 0; r < NR * PS; r++) pr[r] = 0.0f;
 #pragma unroll 16
             for (int kk = 0; kk < SB / 2; kk++) {
                 const int k = hh * (SB / 2) + kk;
                 const float m = op[k * (FWD ? OPL : SB) + i];
 #pragma unroll
-                for (int r = 0; r < NR; r++) pr[r] = fmaf(m, acc[r * SB + k], pr[r]);
+                for (int r = 0; r < NR; r++) pr[r * PS + kk % PS] = fmaf(m, acc[r * SB + k], pr[r * PS + kk % PS]);
             }
 #pragma unroll
-            for (int r = 0; r < NR; r++) part[(hh * NR + r) * SB + i] = pr[r];
+            for (int r = 0; r < NR; r++) {
+                float v = pr[r * PS];
+                if constexpr (PS > 1) v = (pr[r * PS] + pr[r * PS + 1]) + (pr[r * PS + 2] + pr[r * PS + 3]);
+                part[(hh * NR + r) * SB + i] = v;
+            }
         }
         __syncthreads();
         for (int idx = tid; idx < NR * SB; idx += GT) {
