@@ -7,38 +7,50 @@
 //   backward acc_j = y_j + sum_{K>j} s_K^T S[K][j],  s_j = X_j^T acc_j,  x_j = -s_j
 // with, for the diagonal block D of tile j,
 //   Y = (I - U)^-1             U: D's strict upper storage triangle (the
-//                              negated multipliers), by the left recurrence
-//                              applied to an identity;
+//                              negated multipliers);
 //   X = (diag(D_kk)^-1 - L)^-1 L: D's strict lower storage triangle (the U
-//                              factor of M), D_kk = -1/d as stored, by the top
-//                              recurrence applied to an identity.
+//                              factor of M), D_kk = -1/d as stored.
 // Within a tile the sequential 128-step chain becomes one 128 x 128
-// matrix-vector product over all 256 threads.
+// matrix-vector product.  The operators are built blockwise in shared memory:
+// the four 32 x 32 diagonal blocks by one warp each (a lane per column, the
+// 32-step recurrence in registers), then the blocks beside the diagonal by
+// products, for upper T = [A B; 0 C]: T^-1 = [A^-1, -A^-1 B C^-1; 0, C^-1]
+// (lower alike), first for the 32-blocks of each 64 x 64 half, then for the
+// 64 x 64 block.
 //
-// Each sweep is ONE persistent launch, one CTA per SM.  A CTA takes tiles in
-// ticket order (forward 0, 1, 2, ...; backward from the last tile down) and,
-// for its tile j:
-//   1. starts streaming the factor blocks S[K][j] of every source tile K
-//      (forward K < j, backward K > j) through a cp.async ring of 32-row
-//      stages (5 to 7 deep), so a whole source tile and more is in flight;
-//   2. inverts its own diagonal block into shared memory (Y or X: no
-//      separate launch, no global workspace for the operators) when it
-//      would otherwise wait for a source that is not published yet;
-//   3. for each source tile waits for its published values (one poll loop
-//      over the tile's (value, tag) pairs), then adds its contributions;
-//   4. forms acc_j, multiplies by the operator, publishes its own values.
+// Each sweep is ONE persistent launch, one CTA per SM, taking work items in
+// ticket order.  In sweep order (forward: tiles 0, 1, ...; backward: from the
+// last tile down) tile t has the sources u = 0 .. t-1.  With a chunk size Q
+// (0: no chunks), the sources [0, M Q), M = floor((t - 1) / Q), form M chunk
+// items of Q sources that each publish the partial sum of their sources; the
+// tile's finisher item takes the remaining sources [M Q, t), adds the chunks'
+// sums in chunk order, builds the tile's operator and publishes the tile's
+// values.  Long source ranges are thus streamed by several SMs at once
+// instead of one.  Items are numbered tile by tile (tile t's chunks, then its
+// finisher), and every item waits only on items with lower numbers, whose
+// tickets were taken earlier by running CTAs: progress is guaranteed even when
+// not every CTA is resident.  Every wait is bounded nonetheless (250 ms by
+// %globaltimer); a CTA that gives up records the error, writes NaN for its
+// item and still publishes it, so no other CTA waits on it.
+//
+// Per item the CTA streams the factor blocks S[K][j] of its sources through a
+// cp.async ring of 32-row stages (6 to 7 deep) and, per source, completes the
+// source's published values (prefetched one source ahead: already published
+// sources cost no round trip) before adding its contributions.  The finisher
+// keeps its last source's four stages in the ring: it forms everything else
+// first (the input, the chunks' sums and its other sources), builds the
+// operator when it would otherwise wait, and only then waits for the last
+// source, so a step of the tile chain costs one 128 x 128 product for the last
+// source and one for the operator.
+//
 // Published values are 64-bit pairs (tag << 32 | float bits), written with
 // relaxed stores and read with relaxed loads: a pair is valid on its own, so a
 // consumer needs one L2 round trip (no flag, then data).  The forward sweep
-// tags with 1, the backward sweep with 2 into the same array (it is cleared
-// before the forward sweep), and the backward sweep reads its input y_j
-// there.  A CTA only waits on tiles whose tickets were taken before its own
-// by running CTAs, so progress is guaranteed even when not every CTA is
-// resident; every wait is bounded nonetheless (250 ms by %globaltimer), and a
-// CTA that gives up records the error, writes NaN for its tile and still
-// publishes it, so no other CTA waits on it.  The summation order is fixed
-// (sources in order, rows in order, a fixed two-way reduction), so results
-// are deterministic.
+// tags with 1, the backward sweep with 2 into the same array (cleared before
+// the forward sweep); the backward sweep reads its input y_j there.  The
+// summation order is fixed (sources in order, rows in order, chunks in order,
+// fixed two-way reductions), so results are deterministic whichever CTA runs
+// an item.
 #include <algorithm>
 
 #include "gesl_common.cuh"
@@ -48,15 +60,24 @@ namespace {
 
 using namespace gesl;
 
-constexpr int ICH = 32;        // chunk of the inverse recurrences
 constexpr int RS = 32;         // factor rows per ring stage
 constexpr int SPT = SB / RS;   // stages per source tile
 constexpr int STAGE_FLOATS = RS * SB;
-constexpr int OPL = SB + 1;              // row stride of the forward operator (its rows are recurrence chains)
-constexpr int kOpFloats = SB * OPL;
-constexpr int kScratch = 2 * 32 * SB;     // two chunks of the diagonal block (2 x 32 x 128), later the reductions
-constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;  // a bounded wait gives up after 250 ms
+constexpr int LDY = SB + 4;    // row stride of the operator
+constexpr int kOpFloats = SB * LDY;
+// Pieces of the diagonal block (row strides 36 and 68 keep the products free
+// of bank conflicts): the four 32 x 32 diagonal blocks, the two 32 x 32 blocks
+// beside the diagonal inside each 64 x 64 half, and the 64 x 64 block joining
+// the halves.  The region is reused for the products' temporaries and, once
+// the operator is built, for the tile's sums.
+constexpr int L32 = 36, L64 = 68;
+constexpr int kMidOff = 4 * 32 * L32;
+constexpr int kTopOff = kMidOff + 2 * 32 * L32;
+constexpr int kScrFloats = kTopOff + 64 * L64;
+constexpr int kPieceVecs = (4 * 32 * 32 + 2 * 32 * 32 + 64 * 64) / 4;  // 16-byte vectors of the pieces
+constexpr unsigned long long kWaitLimitNs = 250ull * 1000 * 1000;     // a bounded wait gives up after 250 ms
 constexpr unsigned kTagFwd = 1, kTagBwd = 2, kTagNever = 0x7fff0000u;
+static_assert(kPieceVecs % GT == 0, "piece loads");
 
 __device__ __forceinline__ void cp_async16(float* smem, const float* gmem, int src_bytes) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -66,128 +87,194 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Rows [r0, r0 + rows) x columns [k0, k0 + cols) of the diagonal block d
-// (cols a multiple of 4; entries outside the kb x kb block read as 0) into
-// buf (row stride cols) by 16-byte asynchronous copies, committed as one group.
-__device__ __forceinline__ void load_block(const float* __restrict__ d, int lda, int kb, int r0, int rows, int k0,
-                                           int cols, float* buf) {
-    const int q4 = cols / 4;
-    for (int idx = threadIdx.x; idx < rows * q4; idx += GT) {
-        const int rr = idx / q4, cc = (idx - rr * q4) * 4;
-        const int r = r0 + rr, c = k0 + cc, rem = kb - c;
-        const int bytes = (r < kb && rem > 0) ? (rem >= 4 ? 16 : 4 * rem) : 0;
-        cp_async16(buf + rr * cols + cc, bytes > 0 ? d + (size_t)r * lda + c : d, bytes);
+// Work items of one sweep: chunk items of tile t (t >= 1) and the number of
+// items before tile t (the finishers of the tiles before it plus their chunks).
+__host__ __device__ __forceinline__ int chunks_of(int t, int q) { return (q > 0 && t >= 1) ? (t - 1) / q : 0; }
+__host__ __device__ __forceinline__ long long chunks_before(int t, int q) {
+    if (q <= 0 || t <= 1) return 0;
+    const long long v = t - 1, a = v / q, b = v - a * q;  // sum_{w < v} floor(w / q)
+    return q * a * (a - 1) / 2 + a * b;
+}
+__host__ __device__ __forceinline__ long long items_before(int t, int q) { return t + chunks_before(t, q); }
+
+// D[r][c .. c+3] with the identity outside the kb x kb block.
+__device__ __forceinline__ float4 load4_block(const float* __restrict__ d, int lda, int kb, int r, int c) {
+    if (r < kb && c + 3 < kb) return *reinterpret_cast<const float4*>(d + (size_t)r * lda + c);
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int cc = c + e;
+        v[e] = (r < kb && cc < kb) ? d[(size_t)r * lda + cc] : (r == cc ? 1.0f : 0.0f);
     }
-    cp_commit();
+    return make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// X = (diag(D_kk)^-1 - L)^-1 for the diagonal block d (kb valid rows and
-// columns; the rest of the 128 x 128 block is the identity) into op (row
-// stride SB): the top recurrence applied to the identity, every column at
-// once (columns are independent).  Per 32-row chunk of D (double-buffered
-// asynchronous copies, the next chunk in flight): one thread per column runs
-// the chunk's 32-step recurrence in registers, then all threads apply the
-// chunk to the rows below it.  scr: 2 x 128 x 32 floats.  Waiting for its
-// copies also completes any copies the calling thread issued before.
-__device__ void inv_top_full(const float* __restrict__ d, int lda, int kb, float* scr, float* op) {
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < SB * SB; idx += GT) op[idx] = (idx / SB == idx % SB) ? 1.0f : 0.0f;
-    load_block(d, lda, kb, 0, SB, 0, ICH, scr);
-    for (int r0 = 0, ch = 0; r0 < SB; r0 += ICH, ch++) {
-        const int nr = SB - r0;
-        float* dch = scr + (ch & 1) * (SB * ICH);  // rows r0.. of columns [r0, r0 + 32), SB x ICH
-        if (r0 + ICH < SB) {
-            load_block(d, lda, kb, r0 + ICH, nr - ICH, r0 + ICH, ICH, scr + ((ch + 1) & 1) * (SB * ICH));
-            cp_wait<1>();
-        } else {
-            cp_wait<0>();
+// The pieces of the diagonal block d that the operator needs, into scr:
+// forward the upper ones (D01, D23 beside the diagonal, D[0:64][64:128]),
+// backward the lower ones (D10, D32, D[64:128][0:64]).
+template <bool FWD>
+__device__ void load_pieces(const float* __restrict__ d, int lda, int kb, float* scr) {
+    constexpr int NV = kPieceVecs / GT;
+    float4 v[NV];
+    int dst[NV];
+#pragma unroll
+    for (int it = 0; it < NV; it++) {
+        const int idx = threadIdx.x + it * GT;
+        int r, c, o;
+        if (idx < 1024) {  // diagonal blocks
+            const int b = idx >> 8, rr = (idx >> 3) & 31, cq = (idx & 7) * 4;
+            r = 32 * b + rr;
+            c = 32 * b + cq;
+            o = b * 32 * L32 + rr * L32 + cq;
+        } else if (idx < 1536) {  // beside the diagonal inside each half
+            const int i2 = idx - 1024, p = i2 >> 8, rr = (i2 >> 3) & 31, cq = (i2 & 7) * 4;
+            r = FWD ? 64 * p + rr : 64 * p + 32 + rr;
+            c = FWD ? 64 * p + 32 + cq : 64 * p + cq;
+            o = kMidOff + p * 32 * L32 + rr * L32 + cq;
+        } else {  // joining the halves
+            const int i3 = idx - 1536, rr = i3 >> 4, cq = (i3 & 15) * 4;
+            r = FWD ? rr : 64 + rr;
+            c = FWD ? 64 + cq : cq;
+            o = kTopOff + rr * L64 + cq;
         }
-        __syncthreads();
-        if (kb < SB)  // the identity outside the kb x kb block: diagonal entries at and after kb
-            for (int rr = tid; rr < min(nr, ICH); rr += GT)
-                if (r0 + rr >= kb) dch[rr * ICH + rr] = 1.0f;
-        __syncthreads();
-        if (tid < SB) {
-            float x[ICH];
+        v[it] = load4_block(d, lda, kb, r, c);
+        dst[it] = o;
+    }
 #pragma unroll
-            for (int k = 0; k < ICH; k++) x[k] = op[(r0 + k) * SB + tid];
+    for (int it = 0; it < NV; it++) *reinterpret_cast<float4*>(scr + dst[it]) = v[it];
+}
+
+// C = A B for two independent 32 x 32 products (threads 0-127 and 128-255,
+// the caller passes each half its own operands): 2 x 4 outputs per thread.
+__device__ __forceinline__ void mm32(const float* A, int lda, const float* B, int ldb, float* C, int ldc) {
+    const int t = threadIdx.x & 127, r = (t >> 3) * 2, cb = (t & 7) * 4;
+    float acc[2][4];
 #pragma unroll
-            for (int k = 0; k < ICH; k++) {
-                const float xk = x[k] * dch[k * ICH + k];
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 32; k += 4) {
+        float4 av[2], bv[4];
+#pragma unroll
+        for (int i = 0; i < 2; i++) av[i] = *reinterpret_cast<const float4*>(A + (r + i) * lda + k);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) bv[kk] = *reinterpret_cast<const float4*>(B + (k + kk) * ldb + cb);
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+            const float a4[4] = {av[i].x, av[i].y, av[i].z, av[i].w};
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                acc[i][0] = fmaf(a4[kk], bv[kk].x, acc[i][0]);
+                acc[i][1] = fmaf(a4[kk], bv[kk].y, acc[i][1]);
+                acc[i][2] = fmaf(a4[kk], bv[kk].z, acc[i][2]);
+                acc[i][3] = fmaf(a4[kk], bv[kk].w, acc[i][3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+        *reinterpret_cast<float4*>(C + (r + i) * ldc + cb) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+}
+
+// C = A B, 64 x 64 over all 256 threads: 4 x 4 outputs per thread.
+__device__ __forceinline__ void mm64(const float* A, int lda, const float* B, int ldb, float* C, int ldc) {
+    const int r = (threadIdx.x >> 4) * 4, cb = (threadIdx.x & 15) * 4;
+    float acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
+#pragma unroll 4
+    for (int k = 0; k < 64; k += 4) {
+        float4 av[4], bv[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) av[i] = *reinterpret_cast<const float4*>(A + (r + i) * lda + k);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++) bv[kk] = *reinterpret_cast<const float4*>(B + (k + kk) * ldb + cb);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const float a4[4] = {av[i].x, av[i].y, av[i].z, av[i].w};
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                acc[i][0] = fmaf(a4[kk], bv[kk].x, acc[i][0]);
+                acc[i][1] = fmaf(a4[kk], bv[kk].y, acc[i][1]);
+                acc[i][2] = fmaf(a4[kk], bv[kk].z, acc[i][2]);
+                acc[i][3] = fmaf(a4[kk], bv[kk].w, acc[i][3]);
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+        *reinterpret_cast<float4*>(C + (r + i) * ldc + cb) = make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+}
+
+// The tile's operator (Y forward, X backward; row stride LDY) from the pieces
+// in scr (consumed).  Ends with a barrier.
+template <bool FWD>
+__device__ void build_operator(float* scr, float* op) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    if (w < 4) {  // the diagonal 32 x 32 blocks: warp w inverts block w, lane = column
+        const float* db = scr + w * 32 * L32;
+        float x[32];
+#pragma unroll
+        for (int r = 0; r < 32; r++) x[r] = r == lane ? 1.0f : 0.0f;
+        if (FWD) {  // (I - U) x = e_lane, from the last row up
+#pragma unroll
+            for (int k = 31; k > 0; k--) {
+                const float xk = x[k];
+#pragma unroll
+                for (int r = 0; r < k; r++) x[r] = fmaf(db[r * L32 + k], xk, x[r]);
+            }
+        } else {  // (diag(D_kk)^-1 - L) x = e_lane, from the first row down
+#pragma unroll
+            for (int k = 0; k < 32; k++) {
+                const float xk = db[k * L32 + k] * x[k];
                 x[k] = xk;
 #pragma unroll
-                for (int j = k + 1; j < ICH; j++) x[j] = fmaf(xk, dch[j * ICH + k], x[j]);
-            }
-#pragma unroll
-            for (int k = 0; k < ICH; k++) op[(r0 + k) * SB + tid] = x[k];
-        }
-        __syncthreads();
-        if (nr > ICH) {
-            const int c = tid & (SB - 1), g = tid >> 7;
-            float x[ICH];
-#pragma unroll
-            for (int k = 0; k < ICH; k++) x[k] = op[(r0 + k) * SB + c];
-            // four rows at a time: independent FMA chains interleave
-#pragma unroll 4
-            for (int r = r0 + ICH + g; r < SB; r += GT / SB) {
-                float acc = op[r * SB + c];
-                const float* drow = dch + (r - r0) * ICH;
-#pragma unroll
-                for (int k = 0; k < ICH; k++) acc = fmaf(x[k], drow[k], acc);
-                op[r * SB + c] = acc;
+                for (int r = k + 1; r < 32; r++) x[r] = fmaf(db[r * L32 + k], xk, x[r]);
             }
         }
+        float* yb = op + (32 * w) * LDY + 32 * w + lane;
+#pragma unroll
+        for (int r = 0; r < 32; r++) yb[r * LDY] = x[r];
+    } else {  // the 32 x 32 blocks that stay zero: below the diagonal (forward) or above it (backward)
+        for (int idx = tid - 128; idx < 6 * 1024; idx += 128) {
+            const int blk = idx >> 10, e = idx & 1023, rr = e >> 5, cc = e & 31;
+            const int hi = blk < 1 ? 1 : (blk < 3 ? 2 : 3);  // (1,0) (2,0) (2,1) (3,0) (3,1) (3,2)
+            const int lo = blk - (hi * (hi - 1)) / 2;
+            const int rb = FWD ? hi : lo, cb = FWD ? lo : hi;
+            op[(32 * rb + rr) * LDY + 32 * cb + cc] = 0.0f;
+        }
+    }
+    __syncthreads();
+    {  // the 32 x 32 block beside the diagonal of each 64 x 64 half (threads 0-127: half 0)
+        const int o = 64 * (tid >> 7);
+        const float* mid = scr + kMidOff + (tid >> 7) * 32 * L32;
+        float* wt = scr + (tid >> 7) * 32 * L32;  // over the consumed diagonal pieces
+        if (FWD)
+            mm32(mid, L32, op + (o + 32) * LDY + o + 32, LDY, wt, L32);  // D01 Y11
+        else
+            mm32(mid, L32, op + o * LDY + o, LDY, wt, L32);  // D10 X00
+        __syncthreads();
+        if (FWD)
+            mm32(op + o * LDY + o, LDY, wt, L32, op + o * LDY + o + 32, LDY);  // Y01 = Y00 D01 Y11
+        else
+            mm32(op + (o + 32) * LDY + o + 32, LDY, wt, L32, op + (o + 32) * LDY + o, LDY);  // X10 = X11 D10 X00
         __syncthreads();
     }
-}
-
-// Y = (I - U)^-1 for the diagonal block d into op (row stride OPL): the left
-// recurrence applied to the identity, every row at once (rows are
-// independent).  Per 32-column chunk of D (double-buffered asynchronous
-// copies): one thread per row runs the chunk's recurrence in registers, then
-// all threads apply the chunk to the columns after it, one (row, column)
-// element per thread at a time.  scr: 2 x 32 x 128 floats.
-__device__ void inv_left_full(const float* __restrict__ d, int lda, int kb, float* scr, float* op) {
-    const int tid = threadIdx.x;
-    for (int idx = tid; idx < SB * SB; idx += GT) {
-        const int rr = idx / SB, c = idx - rr * SB;
-        op[rr * OPL + c] = (rr == c) ? 1.0f : 0.0f;
-    }
-    load_block(d, lda, kb, 0, ICH, 0, SB, scr);
-    for (int c0 = 0, ch = 0; c0 < SB; c0 += ICH, ch++) {
-        const int nc = SB - c0;
-        float* dch = scr + (ch & 1) * (ICH * SB);  // rows [c0, c0 + 32) of columns c0.., ICH x nc
-        if (c0 + ICH < SB) {
-            load_block(d, lda, kb, c0 + ICH, ICH, c0 + ICH, nc - ICH, scr + ((ch + 1) & 1) * (ICH * SB));
-            cp_wait<1>();
-        } else {
-            cp_wait<0>();
-        }
+    {  // the 64 x 64 block joining the halves
+        const float* top = scr + kTopOff;
+        float* wt = scr;
+        if (FWD)
+            mm64(top, L64, op + 64 * LDY + 64, LDY, wt, L64);
+        else
+            mm64(top, L64, op, LDY, wt, L64);
         __syncthreads();
-        if (tid < SB) {
-            float x[ICH];
-            float* row = op + tid * OPL + c0;
-#pragma unroll
-            for (int k = 0; k < ICH; k++) x[k] = row[k];
-#pragma unroll
-            for (int k = 0; k < ICH; k++)
-#pragma unroll
-                for (int i = k + 1; i < ICH; i++) x[i] = fmaf(x[k], dch[k * nc + i], x[i]);
-#pragma unroll
-            for (int k = 0; k < ICH; k++) row[k] = x[k];
-        }
-        __syncthreads();
-        const int rest = nc - ICH;
-        // four elements at a time: independent FMA chains interleave
-#pragma unroll 4
-        for (int idx = tid; idx < rest * SB; idx += GT) {
-            const int rr = idx / rest, ci = ICH + (idx - rr * rest);
-            const float* row = op + rr * OPL + c0;
-            float acc = row[ci];
-#pragma unroll
-            for (int k = 0; k < ICH; k++) acc = fmaf(row[k], dch[k * nc + ci], acc);
-            op[rr * OPL + c0 + ci] = acc;
-        }
+        if (FWD)
+            mm64(op, LDY, wt, L64, op + 64, LDY);
+        else
+            mm64(op + 64 * LDY + 64, LDY, wt, L64, op + 64 * LDY, LDY);
         __syncthreads();
     }
 }
@@ -208,25 +295,25 @@ __device__ __forceinline__ void st_pair(unsigned long long* p, unsigned tag, flo
 }
 
 // Ring depth per right-hand-side width: as deep as shared memory allows
-// (227 KB per CTA) beside the operator, the scratch and the staged values.
+// (227 KB per CTA) beside the operator, the pieces and the staged values.
 template <int NR>
 __host__ __device__ constexpr int stages() {
     return NR <= 4 ? 7 : 6;
 }
 
-// Published values of one source tile, prefetched into registers: thread t
-// owns entries idx = t + m * GT (q = idx / 128, i = idx % 128) of the tile's
-// NR x 128 block.
+// Published values of one 128-entry block (a source tile's values or a
+// chunk's sums), prefetched into registers: thread t owns entries
+// idx = t + m * GT (q = idx / 128, i = idx % 128) of the NR x 128 block.
 template <int NR>
 struct Pending {
     static constexpr int M = (NR * SB + GT - 1) / GT;
     unsigned long long w[M];
 };
 
-// Issue the relaxed loads of source tile K's pairs (entries this launch does
-// not need read as valid zeros).
+// Issue the relaxed loads of block K's pairs (entries beyond kbK or g read as
+// valid zeros).
 template <int NR>
-__device__ __forceinline__ void prefetch_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, int K,
+__device__ __forceinline__ void prefetch_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, long long K,
                                               int g, int kbK, unsigned tag) {
 #pragma unroll
     for (int m = 0; m < Pending<NR>::M; m++) {
@@ -246,12 +333,12 @@ __device__ __forceinline__ bool all_tagged(const Pending<NR>& pd, unsigned tag) 
     return ok;
 }
 
-// Complete the prefetched values of source tile K: entries not yet carrying
-// `tag` are polled (bounded by kWaitLimitNs; another CTA's error ends the
-// wait too); the values go to ybuf[i*NR + q].  false (CTA-uniform): a wait
-// gave up (here or in another CTA).
+// Complete the prefetched values of block K: entries not yet carrying `tag`
+// are polled (bounded by kWaitLimitNs; another CTA's error ends the wait
+// too); the values go to ybuf[i*NR + q].  false (CTA-uniform): a wait gave up
+// (here or in another CTA).
 template <int NR>
-__device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, int K, int g,
+__device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, long long K, int g,
                              unsigned tag, float* ybuf, int* err) {
     bool ok = true;
 #pragma unroll
@@ -286,46 +373,68 @@ __device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restri
 // One sweep (see the file comment).  FWD: in = b (rows of ldb), out: the
 // published y.  Backward: in = the forward sweep's published y, out: x = -s
 // into xout (rows of ldb) and the published s.  g = right-hand sides of this
-// launch (<= NR).  stall (tests only): the forward sweep's second tile waits
-// for a tag that is never written, so its bounded wait runs out.
-//
-// Per source tile the CTA completes the values it prefetched one tile ahead
-// (already published sources cost no round trip); the tile's operator is
-// computed at the first source that is not yet published (the CTA would wait
-// anyway), or at the end; the tile's input is staged into shared memory by
-// cp.async with the first ring stage.
+// launch (<= NR); q = chunk size (0: none).  pub holds the tiles' values
+// (blocks 0 .. nblk-1) and then the chunks' sums (block nblk + slot).  stall
+// (tests only): the forward sweep's tile 1 waits for a tag that is never
+// written, so its bounded wait runs out.
 template <int NR, bool FWD>
 __global__ void __launch_bounds__(GT, 1)
     k_gesl_sweep(const float* __restrict__ a, int lda, int n, const float* __restrict__ bin, float* __restrict__ xout,
-                 int ldb, unsigned long long* __restrict__ pub, int g, int* __restrict__ ticket,
+                 int ldb, unsigned long long* __restrict__ pub, int g, int q, int* __restrict__ ticket,
                  int* __restrict__ err, int stall) {
     constexpr int STG = stages<NR>();
+    // PS partial sums per right-hand side (rows round-robin) so that one right-hand side's
+    // FMAs form independent chains; combined in a fixed order
+    constexpr int PS = NR == 1 ? 4 : 1;
     extern __shared__ __align__(16) float smem[];
-    float* op = smem;                         // 128 x 128 operator of the tile (Y, row stride OPL; or X)
-    float* scr = op + kOpFloats;              // a chunk of the diagonal block, later the reductions
-    float* ring = scr + kScratch;             // STG x 32 x 128 factor rows
-    float* ybuf = ring + STG * STAGE_FLOATS;  // 128 x NR published values of one source tile
+    float* op = smem;                         // 128 x 128 operator of the tile (row stride LDY)
+    float* scr = op + kOpFloats;              // pieces of the diagonal block, later the tile's sums
+    float* ring = scr + kScrFloats;           // STG x 32 x 128 factor rows
+    float* ybuf = ring + STG * STAGE_FLOATS;  // 128 x NR published values of one block
     float* inb = ybuf + NR * SB;              // NR x 128 input of the tile (b_j or y_j)
-    __shared__ int s_tile;
+    __shared__ int s_item[2];
     const int tid = threadIdx.x;
     const int nblk = (n + SB - 1) / SB;
+    const long long nitems = items_before(nblk, q);
     const unsigned tag = FWD ? kTagFwd : kTagBwd;
     const int c = tid & (SB - 1), h = tid >> 7;  // compute mapping: column c, rows 16h..16h+15 of a stage
     for (;;) {
-        __syncthreads();  // the previous tile's shared data is consumed
-        if (tid == 0) s_tile = atomicAdd(ticket, 1);
+        __syncthreads();  // the previous item's shared data is consumed
+        if (tid == 0) {
+            const long long k = atomicAdd(ticket, 1);
+            int t = -1, m = 0;
+            if (k < nitems) {  // the tile t with items_before(t) <= k < items_before(t + 1)
+                int lo = 0, hi = nblk - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (items_before(mid, q) <= k)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                t = lo;
+                m = (int)(k - items_before(t, q));
+            }
+            s_item[0] = t;
+            s_item[1] = m;
+        }
         __syncthreads();
-        const int t = s_tile;
-        if (t >= nblk) break;
+        const int t = s_item[0], mi = s_item[1];
+        if (t < 0) break;
+        const int nch = chunks_of(t, q);
+        const bool fin = mi == nch;  // the tile's finisher (else chunk mi)
         const int j = FWD ? t : nblk - 1 - t;
         const int c0 = j * SB, kb = min(SB, n - c0);
-        const int nsrc = FWD ? j : nblk - 1 - j;
+        const int u0 = mi * q;                     // first source of the item
+        const int nsrc = (fin ? t : u0 + q) - u0;  // its sources
         const int total = nsrc * SPT;
-        // stage s: rows [32 (s % SPT), +32) of source tile K(s / SPT), columns [c0, c0 + 128)
+        // the finisher's last source stays in the ring and is added after everything else
+        const int nloop = fin ? nsrc - 1 : nsrc;
+        auto src_tile = [&](int si) { return FWD ? u0 + si : nblk - 1 - (u0 + si); };
+        // stage s: rows [32 (s % SPT), +32) of source si = s / SPT, columns [c0, c0 + 128)
         auto issue = [&](int s) {
             const int si = s / SPT, sr = s - si * SPT;
-            const int K = FWD ? si : nblk - 1 - si;
-            const int r0 = K * SB + sr * RS;
+            const int r0 = src_tile(si) * SB + sr * RS;
             float* dst = ring + (s % STG) * STAGE_FLOATS;
 #pragma unroll
             for (int it = 0; it < STAGE_FLOATS / 4 / GT; it++) {
@@ -337,15 +446,16 @@ __global__ void __launch_bounds__(GT, 1)
                 cp_async16(dst + r * SB + cc, src, bytes);
             }
         };
-        // the tile's input: b_j (forward) or the forward sweep's y_j (the low word of its pairs)
-        for (int idx = tid; idx < NR * SB; idx += GT) {
-            const int q = idx / SB, i = idx - q * SB;
-            if (q < g && i < kb) {
-                const float* src = FWD ? bin + (size_t)q * ldb + c0 + i
-                                       : reinterpret_cast<const float*>(pub + ((size_t)j * g + q) * SB + i);
-                cp_async4(inb + idx, src);
-            } else {
-                inb[idx] = 0.0f;
+        if (fin) {  // the tile's input: b_j (forward) or the forward sweep's y_j (the low word of its pairs)
+            for (int idx = tid; idx < NR * SB; idx += GT) {
+                const int qq = idx / SB, i = idx - qq * SB;
+                if (qq < g && i < kb) {
+                    const float* src = FWD ? bin + (size_t)qq * ldb + c0 + i
+                                           : reinterpret_cast<const float*>(pub + ((size_t)j * g + qq) * SB + i);
+                    cp_async4(inb + idx, src);
+                } else {
+                    inb[idx] = 0.0f;
+                }
             }
         }
 #pragma unroll
@@ -354,25 +464,23 @@ __global__ void __launch_bounds__(GT, 1)
             cp_commit();
         }
         const float* d = a + (size_t)c0 * lda + c0;
-        auto invert = [&]() {
-            if (FWD)
-                inv_left_full(d, lda, kb, scr, op);
-            else
-                inv_top_full(d, lda, kb, scr, op);
+        bool have_op = !fin;  // chunks need no operator
+        auto make_op = [&]() {
+            load_pieces<FWD>(d, lda, kb, scr);
+            __syncthreads();
+            build_operator<FWD>(scr, op);
+            have_op = true;
         };
-        bool inverted = false;
-        // PS partial sums per right-hand side (rows round-robin) so that one right-hand side's
-        // FMAs form independent chains; combined in a fixed order at the end of the tile
-        constexpr int PS = NR == 1 ? 4 : 1;
+        if (fin && t == 0) make_op();
         float p[NR * PS];
 #pragma unroll
-        for (int q = 0; q < NR * PS; q++) p[q] = 0.0f;
+        for (int r = 0; r < NR * PS; r++) p[r] = 0.0f;
         bool ok = *(volatile int*)err == 0;
         ok = __syncthreads_and(ok) != 0;
+        const bool never = FWD && stall != 0 && t == 1;  // tile 1's only source is tile 0
         Pending<NR> pd;
         if (nsrc > 0 && ok) {
-            const int K0 = FWD ? 0 : nblk - 1;
-            const bool never = FWD && stall != 0 && j == 1;
+            const int K0 = src_tile(0);
             prefetch_tile<NR>(pd, pub, K0, g, min(SB, n - K0 * SB), never ? kTagNever : tag);
         }
         // contributions of ring stage s (rows sr*32.. of its source tile) to this thread's sums
@@ -385,42 +493,33 @@ __global__ void __launch_bounds__(GT, 1)
                 const float* y = ybuf + (sr * RS + row) * NR;
                 if constexpr (NR % 4 == 0) {
 #pragma unroll
-                    for (int q = 0; q < NR; q += 4) {
-                        const float4 y4 = *reinterpret_cast<const float4*>(y + q);
-                        p[q] = fmaf(y4.x, v, p[q]);
-                        p[q + 1] = fmaf(y4.y, v, p[q + 1]);
-                        p[q + 2] = fmaf(y4.z, v, p[q + 2]);
-                        p[q + 3] = fmaf(y4.w, v, p[q + 3]);
+                    for (int qq = 0; qq < NR; qq += 4) {
+                        const float4 y4 = *reinterpret_cast<const float4*>(y + qq);
+                        p[qq] = fmaf(y4.x, v, p[qq]);
+                        p[qq + 1] = fmaf(y4.y, v, p[qq + 1]);
+                        p[qq + 2] = fmaf(y4.z, v, p[qq + 2]);
+                        p[qq + 3] = fmaf(y4.w, v, p[qq + 3]);
                     }
                 } else {
 #pragma unroll
-                    for (int q = 0; q < NR; q++) p[q * PS + r % PS] = fmaf(y[q], v, p[q * PS + r % PS]);
+                    for (int qq = 0; qq < NR; qq++) p[qq * PS + r % PS] = fmaf(y[qq], v, p[qq * PS + r % PS]);
                 }
             }
         };
+        const unsigned want = never ? kTagNever : tag;
         for (int s = 0; s < total && ok; s++) {
             const int si = s / SPT, sr = s - si * SPT;
-            const int K = FWD ? si : nblk - 1 - si;
             if (sr == 0) {
-                const unsigned want = (FWD && stall != 0 && j == 1 && K == 0) ? kTagNever : tag;
                 __syncthreads();  // every thread is done with the previous source's values
-                if (!inverted && __syncthreads_and(all_tagged<NR>(pd, want)) == 0) {
-                    invert();  // this source is not published yet: the CTA would wait anyway
-                    inverted = true;
-                }
+                if (!have_op && __syncthreads_and(all_tagged<NR>(pd, want)) == 0)
+                    make_op();  // this source is not published yet: the CTA would wait anyway
+                if (si == nloop) break;  // the finisher's last source: added after the rest
+                const int K = src_tile(si);
                 ok = resolve_tile<NR>(pd, pub, K, g, want, ybuf, err);
                 if (!ok) break;
                 if (si + 1 < nsrc) {
-                    const int K1 = FWD ? si + 1 : nblk - 2 - si;
-                    prefetch_tile<NR>(pd, pub, K1, g, min(SB, n - K1 * SB), tag);
-                } else {
-                    // the last source (on the chain's critical path): all of its stages are in
-                    // the ring already (STG > SPT), so one wait and one barrier cover them
-                    cp_wait<0>();
-                    __syncthreads();
-#pragma unroll
-                    for (int r4 = 0; r4 < SPT; r4++) consume(s + r4, r4);
-                    break;
+                    const int K1 = src_tile(si + 1);
+                    prefetch_tile<NR>(pd, pub, K1, g, min(SB, n - K1 * SB), want);
                 }
             }
             cp_wait<STG - 2>();
@@ -430,27 +529,92 @@ __global__ void __launch_bounds__(GT, 1)
             consume(s, sr);
         }
         cp_wait<0>();
-        if (!inverted) invert();
-        // acc = in + the two half sums; res = operator^T acc; published from the two halves of the product
-        float* red = scr;                 // NR x 128: the upper half's sums
-        float* acc = red + NR * SB;       // NR x 128
-        float* part = acc + NR * SB;      // 2 x NR x 128
+        if (!have_op) make_op();
+        // this thread's sums of the sources added so far; the upper half's go to red
+        float* red = scr;             // NR x 128
+        float* acc = red + NR * SB;   // 128 x NR (i * NR + q): the tile's accumulated input
+        float* part = acc + NR * SB;  // 2 x NR x 128
         if constexpr (PS > 1) {
 #pragma unroll
-            for (int q = 0; q < NR; q++) p[q * PS] = (p[q * PS] + p[q * PS + 1]) + (p[q * PS + 2] + p[q * PS + 3]);
+            for (int qq = 0; qq < NR; qq++)
+                p[qq * PS] = (p[qq * PS] + p[qq * PS + 1]) + (p[qq * PS + 2] + p[qq * PS + 3]);
         }
         if (h == 1) {
 #pragma unroll
-            for (int q = 0; q < NR; q++) red[q * SB + c] = p[q * PS];
+            for (int qq = 0; qq < NR; qq++) red[qq * SB + c] = p[qq * PS];
         }
         ok = __syncthreads_and(ok) != 0;
+        if (!fin) {  // a chunk: publish its sums
+            if (h == 0) {
+                unsigned long long* dst = pub + (size_t)(nblk + chunks_before(t, q) + mi) * g * SB;
+#pragma unroll
+                for (int qq = 0; qq < NR; qq++)
+                    if (qq < g && c < kb)
+                        st_pair(dst + (size_t)qq * SB + c, tag,
+                                ok ? p[qq * PS] + red[qq * SB + c] : __int_as_float(0x7fc00000));  // NaN: aborted
+            }
+            continue;
+        }
+        // the finisher: acc = in + the chunks' sums (in chunk order) + its own sources but the last
+        float own[NR];
+#pragma unroll
+        for (int qq = 0; qq < NR; qq++) own[qq] = p[qq * PS] + red[qq * SB + c];
         if (h == 0) {
 #pragma unroll
-            for (int q = 0; q < NR; q++)
-                acc[q * SB + c] = (q < g && c < kb) ? inb[q * SB + c] + p[q * PS] + red[q * SB + c] : 0.0f;
+            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] = inb[qq * SB + c];
         }
-        __syncthreads();
-        {
+        {  // the chunks' sums, CG chunks' loads in flight at a time
+            constexpr int CG = NR == 1 ? 8 : (NR <= 4 ? 4 : 1);
+            const long long base = nblk + chunks_before(t, q);
+            for (int m0 = 0; m0 < nch && ok; m0 += CG) {
+                Pending<NR> pc[CG];
+#pragma unroll
+                for (int e = 0; e < CG; e++)
+                    if (m0 + e < nch) prefetch_tile<NR>(pc[e], pub, base + m0 + e, g, kb, tag);
+#pragma unroll
+                for (int e = 0; e < CG; e++) {
+                    if (m0 + e < nch && ok) {
+                        __syncthreads();  // ybuf is free
+                        ok = resolve_tile<NR>(pc[e], pub, base + m0 + e, g, tag, ybuf, err);
+                        if (h == 0) {
+#pragma unroll
+                            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] += ybuf[c * NR + qq];
+                        }
+                    }
+                }
+            }
+        }
+        if (h == 0) {
+#pragma unroll
+            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] += own[qq];
+        }
+        // the last source: its values, then its four stages (all in the ring: STG > SPT)
+        if (nsrc > 0 && ok) {
+            __syncthreads();  // ybuf is free
+            ok = resolve_tile<NR>(pd, pub, src_tile(nloop), g, want, ybuf, err);
+            if (ok) {
+#pragma unroll
+                for (int r = 0; r < NR * PS; r++) p[r] = 0.0f;
+#pragma unroll
+                for (int r4 = 0; r4 < SPT; r4++) consume(nloop * SPT + r4, r4);
+                if constexpr (PS > 1) {
+#pragma unroll
+                    for (int qq = 0; qq < NR; qq++)
+                        p[qq * PS] = (p[qq * PS] + p[qq * PS + 1]) + (p[qq * PS + 2] + p[qq * PS + 3]);
+                }
+                if (h == 1) {
+#pragma unroll
+                    for (int qq = 0; qq < NR; qq++) red[qq * SB + c] = p[qq * PS];
+                }
+                __syncthreads();
+                if (h == 0) {
+#pragma unroll
+                    for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] += p[qq * PS] + red[qq * SB + c];
+                }
+            }
+        }
+        ok = __syncthreads_and(ok) != 0;
+        {  // res = operator^T acc, from the two halves of the product
             const int i = tid & (SB - 1), hh = tid >> 7;
             float pr[NR * PS];
 #pragma unroll
@@ -458,9 +622,9 @@ __global__ void __launch_bounds__(GT, 1)
 #pragma unroll 16
             for (int kk = 0; kk < SB / 2; kk++) {
                 const int k = hh * (SB / 2) + kk;
-                const float m = op[k * (FWD ? OPL : SB) + i];
+                const float m = op[k * LDY + i];
 #pragma unroll
-                for (int r = 0; r < NR; r++) pr[r * PS + kk % PS] = fmaf(m, acc[r * SB + k], pr[r * PS + kk % PS]);
+                for (int r = 0; r < NR; r++) pr[r * PS + kk % PS] = fmaf(m, acc[k * NR + r], pr[r * PS + kk % PS]);
             }
 #pragma unroll
             for (int r = 0; r < NR; r++) {
@@ -471,12 +635,12 @@ __global__ void __launch_bounds__(GT, 1)
         }
         __syncthreads();
         for (int idx = tid; idx < NR * SB; idx += GT) {
-            const int q = idx / SB, i = idx - q * SB;
-            if (q < g && i < kb) {
-                const float v = ok ? part[q * SB + i] + part[(NR + q) * SB + i]
+            const int qq = idx / SB, i = idx - qq * SB;
+            if (qq < g && i < kb) {
+                const float v = ok ? part[qq * SB + i] + part[(NR + qq) * SB + i]
                                    : __int_as_float(0x7fc00000);  // NaN marks an aborted solve
-                if (!FWD) xout[(size_t)q * ldb + c0 + i] = -v;
-                st_pair(pub + ((size_t)j * g + q) * SB + i, tag, v);
+                if (!FWD) xout[(size_t)qq * ldb + c0 + i] = -v;
+                st_pair(pub + ((size_t)j * g + qq) * SB + i, tag, v);
             }
         }
     }
@@ -485,24 +649,26 @@ __global__ void __launch_bounds__(GT, 1)
 template <int NR>
 constexpr size_t sweep_smem() {
     return sizeof(float) *
-           ((size_t)kOpFloats + kScratch + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
+           ((size_t)kOpFloats + kScrFloats + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
 }
-// a chunk of the diagonal block and the reductions fit in the scratch
-static_assert(2 * SB * ICH <= kScratch && 4 * 16 * SB <= kScratch, "scratch");
+// the tile's sums fit in the pieces' region; the finisher's last source fits in the ring
+static_assert(4 * 16 * SB <= kScrFloats && 64 * L64 <= kMidOff, "scratch");
+static_assert(stages<16>() > SPT && stages<1>() > SPT, "ring");
 static_assert(sweep_smem<1>() <= 227 * 1024 && sweep_smem<4>() <= 227 * 1024 && sweep_smem<16>() <= 227 * 1024,
               "sweep shared memory");
 
 template <int NR>
-int sweeps(const float* a, int lda, int n, float* b, int ldb, int g, unsigned long long* pub, int* tickets, int* err,
-           bool stall, int sms, cudaStream_t st) {
+int sweeps(const float* a, int lda, int n, float* b, int ldb, int g, int q, unsigned long long* pub, int* tickets,
+           int* err, bool stall, int sms, cudaStream_t st) {
     const int nblk = (n + SB - 1) / SB;
-    const int grid = std::min(nblk, sms);
+    const long long items = items_before(nblk, q);
+    const int grid = (int)std::min<long long>(items, sms);
     LP_CUDA(cudaMemsetAsync(tickets, 0, 2 * sizeof(int), st));
-    LP_CUDA(cudaMemsetAsync(pub, 0, sizeof(unsigned long long) * (size_t)nblk * SB * g, st));
-    k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, b, nullptr, ldb, pub, g, tickets, err,
+    LP_CUDA(cudaMemsetAsync(pub, 0, sizeof(unsigned long long) * gesl_pub_pairs(n, g, q), st));
+    k_gesl_sweep<NR, true><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, b, nullptr, ldb, pub, g, q, tickets, err,
                                                                stall ? 1 : 0);
-    k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, nullptr, b, ldb, pub, g, tickets + 1, err,
-                                                                0);
+    k_gesl_sweep<NR, false><<<grid, GT, sweep_smem<NR>(), st>>>(a, lda, n, nullptr, b, ldb, pub, g, q, tickets + 1,
+                                                                err, 0);
     count_launch(2);
     LP_CUDA(cudaGetLastError());
     return LP_OK;
@@ -526,21 +692,25 @@ int gesl_inv_init_attrs() {
     return LP_OK;
 }
 
-// Published-value pairs of one solve: ceil(n / 128) * 128 * min(nrhs, 16).
-size_t gesl_pub_pairs(int n, int nrhs) {
+// Published-value pairs of one solve: the tiles' values and, with chunks of
+// `chunk` sources, the chunks' sums, each ceil(n / 128) x 128 x min(nrhs, 16).
+size_t gesl_pub_pairs(int n, int nrhs, int chunk) {
     const size_t g = nrhs < 16 ? nrhs : 16;
-    return (size_t)((n + SB - 1) / SB) * SB * g;
+    const int nblk = (n + SB - 1) / SB;
+    return (size_t)(nblk + chunks_before(nblk, chunk)) * SB * g;
 }
 
 // Forward + back substitution for nrhs rows of b (overwritten by x), in
-// chunks of at most 16 right-hand sides.  pub: gesl_pub_pairs(n, nrhs) pairs;
-// tickets: 2 ints; err: an error word the caller zeroes and reads (set when a
-// bounded wait gave up; that tile is written as NaN).  pub and tickets are
-// cleared here before every chunk.  stall (tests only): see k_gesl_sweep.
+// chunks of at most 16 right-hand sides.  pub: gesl_pub_pairs(n, nrhs, chunk)
+// pairs; tickets: 2 ints; err: an error word the caller zeroes and reads (set
+// when a bounded wait gave up; that tile is written as NaN).  pub and tickets
+// are cleared here before every group of right-hand sides.  stall (tests
+// only): see k_gesl_sweep.
 int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, unsigned long long* pub,
-                    int* tickets, int* err, bool stall, cudaStream_t st) {
+                    int* tickets, int* err, bool stall, int chunk, cudaStream_t st) {
     if (n <= 0 || nrhs <= 0) return LP_OK;
     if (lda % 4 != 0 || !aligned16(a)) return fail(LP_E_INVALID, "gesl: factors need lda % 4 == 0, 16-byte aligned");
+    if (chunk < 0) return fail(LP_E_INVALID, "gesl: negative chunk size");
     int dev = 0, sms = 0;
     LP_CUDA(cudaGetDevice(&dev));
     LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -549,11 +719,11 @@ int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs,
         float* bb = b + (size_t)r0 * ldb;
         const bool stall_here = stall && r0 == 0;
         if (g == 1)
-            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
+            LP_CHECK(sweeps<1>(a, lda, n, bb, ldb, g, chunk, pub, tickets, err, stall_here, sms, st));
         else if (g <= 4)
-            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
+            LP_CHECK(sweeps<4>(a, lda, n, bb, ldb, g, chunk, pub, tickets, err, stall_here, sms, st));
         else
-            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, pub, tickets, err, stall_here, sms, st));
+            LP_CHECK(sweeps<16>(a, lda, n, bb, ldb, g, chunk, pub, tickets, err, stall_here, sms, st));
     }
     return LP_OK;
 }

@@ -448,7 +448,7 @@ int gefa_f32_streamed(lp_ctx* c, const float* hA, float* dA, int n, int lda, int
 }
 
 int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, int ldb, cudaStream_t st) {
-    const size_t pairs = gesl_pub_pairs(n, nrhs);
+    const size_t pairs = gesl_pub_pairs(n, nrhs, kGeslChunk);
     LP_CHECK(c->gw.ensure(sizeof(unsigned long long) * pairs + 4 * sizeof(int)));
     LP_CHECK(c->gerr.ensure(sizeof(int)));
     auto* pub = static_cast<unsigned long long*>(c->gw.ptr);
@@ -456,7 +456,8 @@ int gesl_f32(lp_ctx* c, const float* dLU, int n, int lda, float* dB, int nrhs, i
     const bool stall = c->stall_site == LP_STALL_GESL;
     c->stall_site = stall ? 0 : c->stall_site;
     const int e = prof_begin(c, st);
-    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, pub, tickets, static_cast<int*>(c->gerr.ptr), stall, st));
+    LP_CHECK(launch_gesl_inv(dLU, lda, n, dB, ldb, nrhs, pub, tickets, static_cast<int*>(c->gerr.ptr), stall,
+                             kGeslChunk, st));
     const double nn = n;
     return prof_end(c, st, LP_STAGE_GESL, e, 2.0 * nn * nn * nrhs, 4.0 * nn * nn + 16.0 * nn * nrhs);
 }

@@ -106,12 +106,16 @@ int dgemm_init_attrs();
 int launch_transpose(const float* src, int lds, float* dst, int ldd, int rows, int cols, cudaStream_t s);
 int launch_transpose_f64(const double* src, int lds, double* dst, int ldd, int rows, int cols, cudaStream_t s);
 // Forward + back substitution for nrhs rows of b with the encoded factors:
-// two persistent sweeps per 16 right-hand sides, each CTA inverting its own
-// diagonal block (k_gesl_inv.cu).  pub: gesl_pub_pairs(n, nrhs) 64-bit words,
-// tickets: 2 ints, err: an error word the caller zeroes and reads.
+// two persistent sweeps per 16 right-hand sides, each finisher CTA inverting
+// its own diagonal block, the long source ranges split into chunks of `chunk`
+// source tiles (0: no chunks) streamed by other CTAs (k_gesl_inv.cu).
+// pub: gesl_pub_pairs(n, nrhs, chunk) 64-bit words, tickets: 2 ints, err: an
+// error word the caller zeroes and reads.
 int launch_gesl_inv(const float* a, int lda, int n, float* b, int ldb, int nrhs, unsigned long long* pub,
-                    int* tickets, int* err, bool stall, cudaStream_t st);
-size_t gesl_pub_pairs(int n, int nrhs);
+                    int* tickets, int* err, bool stall, int chunk, cudaStream_t st);
+size_t gesl_pub_pairs(int n, int nrhs, int chunk);
+// Chunk size of the substitution sweeps when the caller's workspace allows it.
+constexpr int kGeslChunk = 32;
 int gesl_inv_init_attrs();
 // FP64 refinement pieces (see k_ir.cu).
 int launch_residual_f64(const float* a, int lda, int n, const double* x, int ldx, const double* b, int ldb,

@@ -222,12 +222,16 @@ int lp_gesl_dev(lp_ctx* ctx, const float* dLU, int n, int lda, float* dB, int nr
  * This entry point allocates nothing and needs no lp_ctx.  It runs the same
  * two persistent sweeps as lp_gesl_dev, whose only global scratch is the
  * array of values the sweeps publish to one another (one 64-bit word per
- * unknown and right-hand side of a 16-wide chunk); here that array is one
- * fixed device array of 2^19 words (4 MiB, plus 16 bytes of counters) that
- * every GPU which loads the library holds until the process exits, so it
- * accepts only ceil(n / 128) * 128 * min(nrhs, 16) <= 524288 (n <= 32768 with
- * 16 or more right-hand sides, n <= 524288 with one) and returns LP_E_INVALID
- * beyond that.  Unlike lp_gesl_dev it does not wait for the device, so it
+ * unknown and right-hand side of a 16-wide group, plus the partial sums of
+ * the chunk items that stream the late tiles' long source ranges); here that
+ * array is one fixed device array of 2^19 words (4 MiB, plus 16 bytes of
+ * counters) that every GPU which loads the library holds until the process
+ * exits.  Where the chunks' sums fit beside the values the result is
+ * bit-identical to lp_gesl_dev's; otherwise the sweeps run without chunk
+ * items (slower at large n, summed in another order), which accepts
+ * ceil(n / 128) * 128 * min(nrhs, 16) <= 524288 (n <= 32768 with 16 or more
+ * right-hand sides, n <= 524288 with one); beyond that it returns
+ * LP_E_INVALID.  Unlike lp_gesl_dev it does not wait for the device, so it
  * cannot report a bounded wait of the sweeps that ran out: the affected
  * solution entries are then NaN.
  * The first call on a device (the current device) looks up the array's

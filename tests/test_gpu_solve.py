@@ -104,6 +104,34 @@ def test_gesl_multi_rhs(ctx, dev, n, nrhs):
         assert np.abs(X[r] - x64).max() <= tol
 
 
+@pytest.mark.parametrize("n,nrhs", [(9000, 1), (9000, 3), (9000, 16), (8324, 17), (4480, 2)])
+def test_gesl_chunked_sources(ctx, dev, n, nrhs):
+    """Sizes where the substitution splits the long source ranges of the late
+    tiles into chunk items (tiles past the 33rd; two chunks past the 65th),
+    ragged n included.  Encoded factors made directly (multipliers up to
+    1e-3, stored diagonal -1/d with d in [1, 2]) keep the oracle fast at these
+    sizes.  Two runs must agree bit for bit: whichever CTA runs a chunk, the
+    summation order is fixed."""
+    rng = np.random.default_rng(n + nrhs)
+    LU = ((rng.random((n, n), dtype=np.float32) - 0.5) * 2e-3).astype(np.float32)
+    LU[np.arange(n), np.arange(n)] = (-1.0 / (1.0 + rng.random(n))).astype(np.float32)
+    B = rng.uniform(-1, 1, (nrhs, n)).astype(np.float32)
+    dLU = dev.put(LU)
+    outs = []
+    for _ in range(2):
+        dB = dev.put(B)
+        ctx.gesl(dLU.data_ptr(), n, n, dB.data_ptr(), nrhs, n)
+        outs.append(dev.get(dB))
+    assert np.array_equal(outs[0].view(np.uint32), outs[1].view(np.uint32))
+    X = outs[0]
+    LU64 = LU.astype(np.float64)
+    for r in range(nrhs):
+        x64 = oracle.gesl_nopvt(LU64, B[r].astype(np.float64))
+        x32 = oracle.gesl_nopvt(LU, B[r])
+        tol = 8 * np.abs(x32 - x64).max() + 64 * FLT_EPS * np.abs(x64).max()
+        assert np.abs(X[r] - x64).max() <= tol
+
+
 def test_gefa_dev_deterministic(ctx, dev):
     n, bs = 1024, 256
     A, _, _, _ = oracle.gen_reference(n)
