@@ -254,7 +254,9 @@ def run_mixed(ctx, lp, torch, stream, dA0, dA, dB64, n, bs, prec, steps, warmup,
         "ir_iters": max(r[0] for r in res), "hpl_resid": max(r[1] for r in res), "hpl_eps": "DBL_EPSILON/2",
         "max_abs_err_vs_fp64_oracle": err,
         "roofline": {"bound": "tensor" if tensor_bound else "hbm",
-                     "kernel": f"k_umma_update<{prec}> (inner stage, tcgen05)",
+                     "kernel": (f"k_umma_pair<{prec}> (inner stage, tcgen05 256 x 256 tiles on CTA pairs)"
+                                if prec == "bf16" or bs <= 512 else
+                                "k_umma_update<fp8, SEG> (inner stage, tcgen05, per-512 K segments)"),
                      "achieved": tfs if tensor_bound else gbs,
                      "peak": tpk if tensor_bound else pk["hbm_gbs"],
                      "unit": "TFLOP/s" if tensor_bound else "GB/s",
@@ -347,7 +349,7 @@ def run_f32emu(ctx, lp, torch, stream, dA0, dA, dB0, dB, dB64, n, bs, steps, war
         "max_abs_err_x": err,
         "hpl_resid": {"eps_flt_half": r32 * 2.0 ** -29, "eps_dbl_half": r32},
         # timed inside a seconds-long factorization: the sustained BF16 figure is the denominator
-        "roofline": {"bound": "tensor", "kernel": "k_umma_update (inner stage, K = 6 bs)",
+        "roofline": {"bound": "tensor", "kernel": "k_umma_pair (inner stage, K = 6 bs)",
                      "achieved": 6 * tf32eq if tf32eq else None, "peak": spk, "unit": "TFLOP/s",
                      "frac": 6 * tf32eq / spk if tf32eq else None,
                      "fp32_equivalent_tflops": tf32eq,

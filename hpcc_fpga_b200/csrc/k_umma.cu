@@ -9,6 +9,9 @@
 // walks 128 x TN C tiles (in groups of 16 tile rows, so that the CTAs in
 // flight share their A and B tiles in L2); TN = 256 where the column range allows it (half the operand
 // bytes per flop of TN = 128, which matters once K is long), else 128.
+// Where both ranges are multiples of 256, k_umma_pair (further down) runs the
+// same update with 256 x 256 tiles over CTA pairs (cta_group::2): a third less
+// operand traffic per flop than the 128 x 256 tile.
 //   warp 0      TMA producer: A and B tiles (128-byte swizzle) into a
 //               STAGES-deep shared-memory ring;
 //   warp 1      one elected thread issues tcgen05.mma (kind::f16 for BF16,
@@ -27,6 +30,8 @@
 // code in *err, raises the CTA's abort flag, stops issuing work, lets its own
 // copies / MMAs in flight finish (bounded again), and the CTA frees its
 // tensor memory and returns; the host reports LP_E_TIMEOUT.
+#include <algorithm>
+
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -466,6 +471,287 @@ __global__ void __launch_bounds__(UT, 1) k_umma_update(const __grid_constant__ C
     }
 }
 
+// ---- CTA pairs (tcgen05 cta_group::2) ------------------------------------------
+// The same update with 256 x 256 tiles over a pair of CTAs (a cluster of two):
+// each CTA stages its own 128 rows of A and its own 128 of the tile's 256
+// columns of B (32 KB per K step instead of 48 KB for a 128 x 256 tile on one
+// SM, so a third less operand traffic from L2 per flop), the even CTA's one
+// elected thread issues M = 256 MMAs that read both CTAs' halves, and each
+// CTA's tensor memory accumulates its own 128 rows of the tile.  Each CTA's
+// TMA loads fill only its own shared memory; they complete on the even CTA's
+// stage barrier, whose expected bytes cover both halves.  The even CTA's MMA commits
+// arrive on both CTAs' barriers (stage free, accumulator full, done); both
+// epilogues arrive on the even CTA's accumulator-free barrier.  Every wait is
+// bounded as in the one-CTA kernel.
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_index() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_count() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%nclusterid.x;" : "=r"(r));
+    return r;
+}
+// The shared-memory address of the same variable in CTA `rank` of the cluster.
+__device__ __forceinline__ uint32_t map_rank(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tma_load_2d_pair(void* dst, const CUtensorMap* map, uint32_t bar_cluster, int x,
+                                                 int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+        "%4}], [%2];" ::"r"(smem_u32(dst)),
+        "l"(map), "r"(bar_cluster), "r"(x), "r"(y)
+        : "memory");
+}
+template <bool FP8>
+__device__ __forceinline__ void umma_pair(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
+    if (FP8) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+            "l"(ad), "l"(bd), "r"(idesc), "r"(acc));
+    }
+}
+// Arrive on the barrier at this offset in both CTAs of the pair once the MMAs issued so far complete.
+__device__ __forceinline__ void umma_commit_pair(uint64_t* bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+            smem_u32(bar)),
+        "h"((uint16_t)3)
+        : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar_cluster) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(bar_cluster) : "memory");
+}
+
+template <bool FP8>
+__host__ __device__ constexpr uint32_t idesc_pair() {
+    return (1u << 4) | ((FP8 ? 0u : 1u) << 7) | ((FP8 ? 0u : 1u) << 10) | ((uint32_t)(256 >> 3) << 17) |
+           ((uint32_t)(256 >> 4) << 24);
+}
+
+// Pair tile tp -> its C origin (256 x 256), in groups of kGroupRows / 2 pair rows.
+__device__ __forceinline__ void pair_origin(int tp, int tiles_n, int tiles, int m_off, int n_off, int* m0, int* n0) {
+    const int tiles_m = tiles / tiles_n;
+    const int gr = kGroupRows / 2;
+    const int group = tp / (gr * tiles_n);
+    const int first = group * gr;
+    const int rows = min(gr, tiles_m - first);
+    const int local = tp - first * tiles_n;
+    *m0 = m_off + (first + local % rows) * 256;
+    *n0 = n_off + (local / rows) * 256;
+}
+
+template <bool FP8>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(UT, 1)
+    k_umma_pair(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                float* __restrict__ C, int ldc, int m_off, int n_off, int tiles_n, int tiles, int kbytes,
+                const float* __restrict__ scale_a, const float* __restrict__ scale_b, int* __restrict__ err) {
+    constexpr int USTAGES = stages<128>();
+    constexpr int kStageBytes = stage_bytes<128>();  // this CTA's A rows and its half of B's columns
+    constexpr int TN = 256;                          // columns of the tile, all in each CTA's accumulator
+    constexpr int kBlk = TN / 64;
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    uint8_t* ring = smem_raw + (base - raw);
+    float* scratch = reinterpret_cast<float*>(ring + USTAGES * kStageBytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(scratch + UEPI * kScratchFloats);
+    uint64_t* empty = full + USTAGES;
+    uint64_t* acc_full = empty + USTAGES;  // [2] MMA -> both epilogues
+    uint64_t* acc_empty = acc_full + 2;    // [2] both epilogues -> MMA (the even CTA's)
+    uint64_t* done = acc_empty + 2;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    const int cl = (int)cluster_index(), ncl = (int)cluster_count();
+    const int KT = kbytes / UKB;
+    constexpr int kSteps = UKB / 32;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < USTAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&acc_full[b], 1);
+            mbar_init(&acc_empty[b], 2 * UEPI);
+        }
+        mbar_init(done, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)(2 * TN)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::);
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // both CTAs' barriers exist before either signals the other's
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer (both CTAs): this CTA's halves, completing on the even CTA's barrier
+            int it = 0;
+            bool ok = true;
+            for (int tp = cl; tp < tiles && ok; tp += ncl) {
+                int m0, n0;
+                pair_origin(tp, tiles_n, tiles, m_off, n_off, &m0, &n0);
+                for (int kt = 0; kt < KT; kt++, it++) {
+                    const int s = it % USTAGES;
+                    if (!mbar_wait(&empty[s], ((it / USTAGES) & 1) ^ 1, abort_flag)) {
+                        atomicExch(err, kErrEmptyWait);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* sa = ring + s * kStageBytes;
+                    if (rank == 0) mbar_expect_tx(&full[s], 2 * kStageBytes);
+                    const uint32_t bar = map_rank(smem_u32(&full[s]), 0);
+                    const int kx = kt * UKB / (FP8 ? 1 : 2);
+                    tma_load_2d_pair(sa, &map_a, bar, kx, m0 + 128 * (int)rank);
+                    tma_load_2d_pair(sa + kTileBytesA, &map_b, bar, kx, n0 + 128 * (int)rank);
+                }
+            }
+            // let this CTA's copies still in flight land before either CTA can exit: the even
+            // CTA waits for its stage barriers, which count both CTAs' bytes; the odd CTA's
+            // copies complete on those barriers, so after an abort it gives them 100 us
+            if (rank == 0) {
+                for (int j = it - USTAGES < 0 ? 0 : it - USTAGES; j < it; j++) {
+                    volatile int no_abort = 0;
+                    mbar_wait(&full[j % USTAGES], (j / USTAGES) & 1, &no_abort);
+                }
+            } else if (!ok) {
+                const uint64_t t0 = global_ns();
+                while (global_ns() - t0 < 100000ull) __nanosleep(1000);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {  // MMA issuer for the pair
+            constexpr uint32_t idesc = idesc_pair<FP8>();
+            int it = 0, i = 0;
+            bool ok = true;
+            for (int tp = cl; tp < tiles && ok; tp += ncl, i++) {
+                const int b = i & 1;
+                if (!mbar_wait(&acc_empty[b], ((i >> 1) & 1) ^ 1, abort_flag)) {
+                    atomicExch(err, kErrEmptyWait);
+                    *abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * TN);
+                for (int kt = 0; kt < KT; kt++, it++) {
+                    const int s = it % USTAGES;
+                    if (!mbar_wait(&full[s], (it / USTAGES) & 1, abort_flag)) {
+                        atomicExch(err, kErrFullWait);
+                        *abort_flag = 1;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(ring + s * kStageBytes);
+                    const uint32_t sb = sa + kTileBytesA;
+#pragma unroll
+                    for (int j = 0; j < kSteps; j++)
+                        umma_pair<FP8>(acc, desc_sw128(sa + 32 * j), desc_sw128(sb + 32 * j), idesc,
+                                       (kt | j) ? 1u : 0u);
+                    umma_commit_pair(&empty[s]);
+                }
+                if (ok) umma_commit_pair(&acc_full[b]);
+            }
+            umma_commit_pair(done);  // tracks every MMA issued above, also on the abort path
+        }
+    } else {  // epilogue (both CTAs): this CTA's 128 rows of the tile
+        const int ew = warp - 2;
+        const int quarter = warp & 3;
+        const int half = ew >> 2;
+        float* scr = scratch + ew * kScratchFloats;
+        const uint32_t acc_empty_even[2] = {map_rank(smem_u32(&acc_empty[0]), 0), map_rank(smem_u32(&acc_empty[1]), 0)};
+        int i = 0;
+        for (int tp = cl; tp < tiles; tp += ncl, i++) {
+            const int b = i & 1;
+            int m0, n0;
+            pair_origin(tp, tiles_n, tiles, m_off, n_off, &m0, &n0);
+            const int r0 = m0 + 128 * (int)rank + quarter * 32, c0 = n0 + half * (TN / 2);
+            float cv[2][32];
+#pragma unroll
+            for (int blk = 0; blk < 2; blk++)
+#pragma unroll
+                for (int r = 0; r < 32; r++) cv[blk][r] = C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane];
+            const bool got = mbar_wait(&acc_full[b], (i >> 1) & 1, abort_flag);
+            if (!__all_sync(0xffffffffu, got)) {
+                if (lane == 0) atomicExch(err, kErrDoneWait);
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            const float sc = (scale_a != nullptr) ? scale_a[(m0 + 128 * (int)rank) >> 9] * scale_b[n0 >> 9] : 1.0f;
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * TN + half * (TN / 2));
+#pragma unroll
+            for (int blk = 0; blk < kBlk; blk++) {
+                uint32_t a[32];
+                tmem_ld32(taddr + 32 * blk, a);
+                tmem_wait_ld();
+                if (blk == kBlk - 1) {
+                    tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive_cluster(acc_empty_even[b]);
+                }
+#pragma unroll
+                for (int c = 0; c < 32; c++) scr[lane * 33 + c] = __uint_as_float(a[c]);
+                __syncwarp();
+#pragma unroll
+                for (int r = 0; r < 32; r++) {
+                    const float v = fmaf(sc, scr[r * 33 + lane], cv[blk & 1][r]);
+                    C[(size_t)(r0 + r) * ldc + c0 + 32 * blk + lane] = v;
+                }
+                if (blk + 2 < kBlk) {
+#pragma unroll
+                    for (int r = 0; r < 32; r++)
+                        cv[blk & 1][r] = C[(size_t)(r0 + r) * ldc + c0 + 32 * (blk + 2) + lane];
+                }
+                __syncwarp();
+            }
+        }
+    }
+    __syncwarp();
+    {  // every MMA of the pair has completed (the even CTA's commit arrives here too)
+        volatile int no_abort = 0;
+        if (!mbar_wait(done, 0, &no_abort)) {
+            if (threadIdx.x == 0) atomicExch(err, kErrDoneWait);
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    cluster_sync();  // neither CTA leaves while the other may still signal its barriers
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)(2 * TN)));
+    }
+}
+
 // ---- host side ---------------------------------------------------------------
 
 // The driver's tensor-map encoder, looked up through the runtime so the
@@ -520,6 +806,10 @@ int umma_init_attrs() {
                                  (int)umma_smem<256>()));
     LP_CUDA(cudaFuncSetAttribute(k_umma_update<true, 128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)umma_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_pair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<128>()));
+    LP_CUDA(cudaFuncSetAttribute(k_umma_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)umma_smem<128>()));
     return LP_OK;
 }
 
@@ -542,14 +832,15 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     const bool seg = fp8 && k > 512;
     if (seg && k % 512 != 0) return fail(LP_E_INVALID, "umma_update: E4M3 with k > 512 needs k % 512 == 0");
     const int nseg = seg ? k / 512 : 1;
-    // the wide tile where the column range is a multiple of it (the segmented E4M3 form keeps its
-    // per-segment sums in registers: narrow tiles only)
+    // 256 x 256 tiles over CTA pairs where both ranges are multiples of 256 (not the segmented
+    // E4M3 form, which keeps its per-segment sums in registers); else the wide one-CTA tile where
+    // the column range is a multiple of it, else the narrow one
+    const bool pair = !seg && m % 256 == 0 && n % 256 == 0 && m_off % 256 == 0 && n_off % 256 == 0;
     const bool wide = !seg && n % (2 * UN) == 0 && n_off % (2 * UN) == 0;
     const int tn = wide ? 2 * UN : UN;
     CUtensorMap ma, mb;
     LP_CHECK(make_map(&ma, aq, aq_rows, k, fp8, UM));
-    LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8, tn));
-    const int tiles_n = n / tn, tiles = tiles_n * (m / UM);
+    LP_CHECK(make_map(&mb, bq, bq_rows, k, fp8, pair ? UN : tn));
     int dev = 0, sms = 0;
     LP_CUDA(cudaGetDevice(&dev));
     LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -559,6 +850,20 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     // (measured on B200, n = 32768: 8 free SMs +9 %; 16 to 48 no further gain).
     constexpr int kPanelSMs = 8;
     const int usable = sms - kPanelSMs > 1 ? sms - kPanelSMs : 1;
+    if (pair) {
+        const int tiles_n = n / 256, tiles = tiles_n * (m / 256);
+        const int clusters = std::max(1, std::min(tiles, usable / 2));
+        if (fp8)
+            k_umma_pair<true><<<2 * clusters, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n,
+                                                                          tiles, kbytes, scale_a, scale_b, err);
+        else
+            k_umma_pair<false><<<2 * clusters, UT, umma_smem<128>(), st>>>(ma, mb, c, ldc, m_off, n_off, tiles_n,
+                                                                           tiles, kbytes, nullptr, nullptr, err);
+        count_launch();
+        LP_CUDA(cudaGetLastError());
+        return LP_OK;
+    }
+    const int tiles_n = n / tn, tiles = tiles_n * (m / UM);
     const int grid = tiles < usable ? tiles : usable;
     if (seg)
         k_umma_update<true, 128, true><<<grid, UT, umma_smem<128>(), st>>>(

@@ -38,7 +38,9 @@ def q_fp8_rows(torch, L):
     return out
 
 
-@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (256, 384, 256), (640, 512, 512)])
+# 256-aligned shapes run as 256 x 256 tiles over CTA pairs (cta_group::2), the others on one CTA
+@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (256, 384, 256), (640, 512, 512), (256, 256, 128),
+                                    (768, 512, 512), (1024, 1536, 2048)])
 def test_inner_update_tc_bf16(ctx, dev, m, n, bs):
     rng = np.random.default_rng(m + n + bs)
     C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
@@ -53,7 +55,7 @@ def test_inner_update_tc_bf16(ctx, dev, m, n, bs):
     assert np.all(np.abs(got - exact) <= bound)
 
 
-@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (1024, 640, 512)])
+@pytest.mark.parametrize("m,n,bs", [(128, 128, 128), (1024, 640, 512), (512, 768, 512), (256, 256, 128)])
 def test_inner_update_tc_fp8(ctx, dev, m, n, bs):
     rng = np.random.default_rng(3 * m + n + bs)
     C = rng.uniform(-1, 1, (m, n)).astype(np.float32)
