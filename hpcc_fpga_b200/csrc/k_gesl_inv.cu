@@ -34,14 +34,16 @@
 // item and still publishes it, so no other CTA waits on it.
 //
 // Per item the CTA streams the factor blocks S[K][j] of its sources through a
-// cp.async ring of 32-row stages (6 to 7 deep) and, per source, completes the
-// source's published values (prefetched one source ahead: already published
-// sources cost no round trip) before adding its contributions.  The finisher
-// keeps its last source's four stages in the ring: it forms everything else
-// first (the input, the chunks' sums and its other sources), builds the
-// operator when it would otherwise wait, and only then waits for the last
-// source, so a step of the tile chain costs one 128 x 128 product for the last
-// source and one for the operator.
+// cp.async ring of nine 32-row stages and, per source, completes the source's
+// published values (prefetched one source ahead: already published sources
+// cost no round trip) before adding its contributions.  A finisher first
+// builds its operator (the diagonal block's pieces use the ring's space
+// meanwhile), then streams; the ring holds more than two source tiles, so the
+// last source's stages are in flight before the one before it is consumed.
+// The finisher keeps its last source's four stages in the ring, forms
+// everything else first (the input, the chunks' sums, its other sources), and
+// only then waits for the last source, so a step of the tile chain costs one
+// 128 x 128 product for the last source and one for the operator.
 //
 // Published values are 64-bit pairs (tag << 32 | float bits), written with
 // relaxed stores and read with relaxed loads: a pair is valid on its own, so a
@@ -294,11 +296,14 @@ __device__ __forceinline__ void st_pair(unsigned long long* p, unsigned tag, flo
     asm volatile("st.relaxed.gpu.global.b64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
 
-// Ring depth per right-hand-side width: as deep as shared memory allows
-// (227 KB per CTA) beside the operator, the pieces and the staged values.
+// Ring depth: as deep as shared memory allows (227 KB per CTA) beside the
+// operator and the staged values (the diagonal block's pieces use the ring's
+// space while the operator is built).  Nine stages hold more than two source
+// tiles, so a finisher's last source is in flight before the one before it is
+// consumed.
 template <int NR>
 __host__ __device__ constexpr int stages() {
-    return NR <= 4 ? 7 : 6;
+    return 9;
 }
 
 // Published values of one 128-entry block (a source tile's values or a
@@ -388,8 +393,8 @@ __global__ void __launch_bounds__(GT, 1)
     constexpr int PS = NR == 1 ? 4 : 1;
     extern __shared__ __align__(16) float smem[];
     float* op = smem;                         // 128 x 128 operator of the tile (row stride LDY)
-    float* scr = op + kOpFloats;              // pieces of the diagonal block, later the tile's sums
-    float* ring = scr + kScrFloats;           // STG x 32 x 128 factor rows
+    float* ring = op + kOpFloats;             // STG x 32 x 128 factor rows
+    float* scr = ring;                        // the diagonal block's pieces while the operator is built
     float* ybuf = ring + STG * STAGE_FLOATS;  // 128 x NR published values of one block
     float* inb = ybuf + NR * SB;              // NR x 128 input of the tile (b_j or y_j)
     __shared__ int s_item[2];
@@ -446,32 +451,26 @@ __global__ void __launch_bounds__(GT, 1)
                 cp_async16(dst + r * SB + cc, src, bytes);
             }
         };
-        if (fin) {  // the tile's input: b_j (forward) or the forward sweep's y_j (the low word of its pairs)
+        if (fin) {
+            // the tile's input: b_j (forward) or the forward sweep's y_j (the low word of its pairs)
             for (int idx = tid; idx < NR * SB; idx += GT) {
                 const int qq = idx / SB, i = idx - qq * SB;
-                if (qq < g && i < kb) {
-                    const float* src = FWD ? bin + (size_t)qq * ldb + c0 + i
-                                           : reinterpret_cast<const float*>(pub + ((size_t)j * g + qq) * SB + i);
-                    cp_async4(inb + idx, src);
-                } else {
-                    inb[idx] = 0.0f;
-                }
+                inb[idx] = (qq < g && i < kb)
+                               ? (FWD ? bin[(size_t)qq * ldb + c0 + i]
+                                      : __uint_as_float((unsigned)ld_pair(pub + ((size_t)j * g + qq) * SB + i)))
+                               : 0.0f;
             }
+            // the operator first: its pieces use the ring's space, and the finisher then holds
+            // it while the ring streams the sources
+            load_pieces<FWD>(a + (size_t)c0 * lda + c0, lda, kb, scr);
+            __syncthreads();
+            build_operator<FWD>(scr, op);
         }
 #pragma unroll
         for (int s = 0; s < STG - 1; s++) {
             if (s < total) issue(s);
             cp_commit();
         }
-        const float* d = a + (size_t)c0 * lda + c0;
-        bool have_op = !fin;  // chunks need no operator
-        auto make_op = [&]() {
-            load_pieces<FWD>(d, lda, kb, scr);
-            __syncthreads();
-            build_operator<FWD>(scr, op);
-            have_op = true;
-        };
-        if (fin && t == 0) make_op();
         float p[NR * PS];
 #pragma unroll
         for (int r = 0; r < NR * PS; r++) p[r] = 0.0f;
@@ -511,8 +510,6 @@ __global__ void __launch_bounds__(GT, 1)
             const int si = s / SPT, sr = s - si * SPT;
             if (sr == 0) {
                 __syncthreads();  // every thread is done with the previous source's values
-                if (!have_op && __syncthreads_and(all_tagged<NR>(pd, want)) == 0)
-                    make_op();  // this source is not published yet: the CTA would wait anyway
                 if (si == nloop) break;  // the finisher's last source: added after the rest
                 const int K = src_tile(si);
                 ok = resolve_tile<NR>(pd, pub, K, g, want, ybuf, err);
@@ -528,12 +525,13 @@ __global__ void __launch_bounds__(GT, 1)
             cp_commit();
             consume(s, sr);
         }
-        cp_wait<0>();
-        if (!have_op) make_op();
-        // this thread's sums of the sources added so far; the upper half's go to red
-        float* red = scr;             // NR x 128
-        float* acc = red + NR * SB;   // 128 x NR (i * NR + q): the tile's accumulated input
-        float* part = acc + NR * SB;  // 2 x NR x 128
+        if (!fin) cp_wait<0>();  // (a finisher's last source may still be in flight)
+        // this thread's sums of the sources added so far; the upper half's go to red.  The sums
+        // use two ring slots whose stages were consumed (the finisher's last source occupies
+        // the four slots before them)
+        float* red = ring + (total % STG) * STAGE_FLOATS;  // NR x 128
+        float* acc = red + NR * SB;                         // 128 x NR (i * NR + q): the tile's accumulated input
+        float* part = ring + ((total + 1) % STG) * STAGE_FLOATS;  // 2 x NR x 128
         if constexpr (PS > 1) {
 #pragma unroll
             for (int qq = 0; qq < NR; qq++)
@@ -592,6 +590,8 @@ __global__ void __launch_bounds__(GT, 1)
         if (nsrc > 0 && ok) {
             __syncthreads();  // ybuf is free
             ok = resolve_tile<NR>(pd, pub, src_tile(nloop), g, want, ybuf, err);
+            cp_wait<0>();
+            __syncthreads();
             if (ok) {
 #pragma unroll
                 for (int r = 0; r < NR * PS; r++) p[r] = 0.0f;
@@ -613,6 +613,7 @@ __global__ void __launch_bounds__(GT, 1)
                 }
             }
         }
+        cp_wait<0>();  // nothing of this item stays in flight (also after a wait that gave up)
         ok = __syncthreads_and(ok) != 0;
         {  // res = operator^T acc, from the two halves of the product
             const int i = tid & (SB - 1), hh = tid >> 7;
@@ -648,12 +649,11 @@ __global__ void __launch_bounds__(GT, 1)
 
 template <int NR>
 constexpr size_t sweep_smem() {
-    return sizeof(float) *
-           ((size_t)kOpFloats + kScrFloats + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
+    return sizeof(float) * ((size_t)kOpFloats + (size_t)stages<NR>() * STAGE_FLOATS + 2 * (size_t)NR * SB);
 }
-// the tile's sums fit in the pieces' region; the finisher's last source fits in the ring
-static_assert(4 * 16 * SB <= kScrFloats && 64 * L64 <= kMidOff, "scratch");
-static_assert(stages<16>() > SPT && stages<1>() > SPT, "ring");
+// the pieces fit in the ring; the tile's sums fit in two slots beside the last source's four
+static_assert(kScrFloats <= 9 * STAGE_FLOATS && 64 * L64 <= kMidOff, "scratch");
+static_assert(2 * 16 * SB <= STAGE_FLOATS && stages<1>() >= 2 * SPT + 1, "ring");
 static_assert(sweep_smem<1>() <= 227 * 1024 && sweep_smem<4>() <= 227 * 1024 && sweep_smem<16>() <= 227 * 1024,
               "sweep shared memory");
 
