@@ -329,15 +329,6 @@ __device__ __forceinline__ void prefetch_tile(Pending<NR>& pd, const unsigned lo
     }
 }
 
-// true when every prefetched entry of the calling thread carries `tag`.
-template <int NR>
-__device__ __forceinline__ bool all_tagged(const Pending<NR>& pd, unsigned tag) {
-    bool ok = true;
-#pragma unroll
-    for (int m = 0; m < Pending<NR>::M; m++) ok = ok && (unsigned)(pd.w[m] >> 32) == tag;
-    return ok;
-}
-
 // Complete the prefetched values of block K: entries not yet carrying `tag`
 // are polled (bounded by kWaitLimitNs; another CTA's error ends the wait
 // too); the values go to ybuf[i*NR + q].  false (CTA-uniform): a wait gave up
