@@ -333,6 +333,31 @@ __device__ __forceinline__ void prefetch_tile(Pending<NR>& pd, const unsigned lo
 // are polled (bounded by kWaitLimitNs; another CTA's error ends the wait
 // too); the values go to ybuf[i*NR + q].  false (CTA-uniform): a wait gave up
 // (here or in another CTA).
+// The value of the pair at src once it carries `tag`: w is its prefetched
+// word, polled again while stale (bounded by kWaitLimitNs; another CTA's error
+// ends the wait too, and ok turns false).
+__device__ __forceinline__ float complete_pair(unsigned long long w, const unsigned long long* src, unsigned tag,
+                                               int* err, bool& ok) {
+    if ((unsigned)(w >> 32) != tag && ok) {
+        const unsigned long long t0 = global_ns();
+        for (;;) {
+            __nanosleep(32);
+            w = ld_pair(src);
+            if ((unsigned)(w >> 32) == tag) break;
+            if (*(volatile int*)err != 0) {
+                ok = false;
+                break;
+            }
+            if (global_ns() - t0 > kWaitLimitNs) {
+                atomicExch(err, 1);
+                ok = false;
+                break;
+            }
+        }
+    }
+    return __uint_as_float((unsigned)w);
+}
+
 template <int NR>
 __device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restrict__ pub, long long K, int g,
                              unsigned tag, float* ybuf, int* err) {
@@ -342,26 +367,7 @@ __device__ bool resolve_tile(Pending<NR>& pd, const unsigned long long* __restri
         const int idx = threadIdx.x + m * GT;
         if (idx >= NR * SB) continue;
         const int q = idx / SB, i = idx - q * SB;
-        unsigned long long w = pd.w[m];
-        if ((unsigned)(w >> 32) != tag && ok) {
-            const unsigned long long* src = pub + ((size_t)K * g + q) * SB + i;
-            const unsigned long long t0 = global_ns();
-            for (;;) {
-                __nanosleep(32);
-                w = ld_pair(src);
-                if ((unsigned)(w >> 32) == tag) break;
-                if (*(volatile int*)err != 0) {
-                    ok = false;
-                    break;
-                }
-                if (global_ns() - t0 > kWaitLimitNs) {
-                    atomicExch(err, 1);
-                    ok = false;
-                    break;
-                }
-            }
-        }
-        ybuf[i * NR + q] = __uint_as_float((unsigned)w);
+        ybuf[i * NR + q] = complete_pair(pd.w[m], pub + ((size_t)K * g + q) * SB + i, tag, err, ok);
     }
     return __syncthreads_and(ok) != 0;
 }
@@ -544,38 +550,52 @@ __global__ void __launch_bounds__(GT, 1)
             }
             continue;
         }
-        // the finisher: acc = in + the chunks' sums (in chunk order) + its own sources but the last
+        // the finisher: acc = (in + the chunks' sums) + its own sources but the last
         float own[NR];
 #pragma unroll
         for (int qq = 0; qq < NR; qq++) own[qq] = p[qq * PS] + red[qq * SB + c];
-        if (h == 0) {
-#pragma unroll
-            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] = inb[qq * SB + c];
-        }
-        {  // the chunks' sums, CG chunks' loads in flight at a time
+        if (nch > 0 && ok) {
+            // the chunks' sums: each thread adds up its entries over the chunks in chunk order
+            // (CG chunks' loads in flight at a time), then one barrier
             constexpr int CG = NR == 1 ? 8 : (NR <= 4 ? 4 : 1);
+            constexpr int M = Pending<NR>::M;
             const long long base = nblk + chunks_before(t, q);
-            for (int m0 = 0; m0 < nch && ok; m0 += CG) {
+            float psum[M];
+#pragma unroll
+            for (int mm = 0; mm < M; mm++) psum[mm] = 0.0f;
+            bool okp = true;
+            for (int m0 = 0; m0 < nch; m0 += CG) {
                 Pending<NR> pc[CG];
 #pragma unroll
                 for (int e = 0; e < CG; e++)
                     if (m0 + e < nch) prefetch_tile<NR>(pc[e], pub, base + m0 + e, g, kb, tag);
 #pragma unroll
                 for (int e = 0; e < CG; e++) {
-                    if (m0 + e < nch && ok) {
-                        __syncthreads();  // ybuf is free
-                        ok = resolve_tile<NR>(pc[e], pub, base + m0 + e, g, tag, ybuf, err);
-                        if (h == 0) {
+                    if (m0 + e < nch) {
 #pragma unroll
-                            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] += ybuf[c * NR + qq];
+                        for (int mm = 0; mm < M; mm++) {
+                            const int idx = tid + mm * GT;
+                            if (idx < NR * SB) {
+                                const int qq = idx / SB, i = idx - qq * SB;
+                                psum[mm] += complete_pair(pc[e].w[mm], pub + ((size_t)(base + m0 + e) * g + qq) * SB + i,
+                                                          tag, err, okp);
+                            }
                         }
                     }
                 }
             }
+            __syncthreads();  // ybuf is free
+#pragma unroll
+            for (int mm = 0; mm < M; mm++) {
+                const int idx = tid + mm * GT;
+                if (idx < NR * SB) ybuf[(idx - (idx / SB) * SB) * NR + idx / SB] = psum[mm];
+            }
+            ok = __syncthreads_and(ok && okp) != 0;
         }
         if (h == 0) {
 #pragma unroll
-            for (int qq = 0; qq < NR; qq++) acc[c * NR + qq] += own[qq];
+            for (int qq = 0; qq < NR; qq++)
+                acc[c * NR + qq] = (inb[qq * SB + c] + (nch > 0 ? ybuf[c * NR + qq] : 0.0f)) + own[qq];
         }
         // the last source: its values, then its four stages (all in the ring: STG > SPT)
         if (nsrc > 0 && ok) {
