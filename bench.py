@@ -726,11 +726,15 @@ def compact_line(full: dict) -> dict:
                 line["large"][p] = _mixed_summary(lg[p])
     ms = full.get("margins")
     if ms:
-        rows = {}
+        # the margins once per n, then per n and precision one [iters, hpl, err] row per margin
+        rows, mlist = {}, {}
         for r in ms:
+            mlist.setdefault(str(r["n"]), [])
+            if sig(r["margin"], 3) not in mlist[str(r["n"])]:
+                mlist[str(r["n"])].append(sig(r["margin"], 3))
             rows.setdefault(f"{r['n']} {r['precision']}", []).append(
-                [sig(r["margin"], 3), r["ir_iters"], sig(r["hpl_resid"], 3), sig(r["max_abs_err"], 2)])
-        line["margins"] = {"cols": ["margin", "iters", "hpl", "err"], **rows}
+                [r["ir_iters"], sig(r["hpl_resid"], 3), sig(r["max_abs_err"], 2)])
+        line["margins"] = {"cols": ["iters", "hpl", "err"], "margin": mlist, **rows}
     em = full.get("f32_bf16x6")
     if em:
         line["f32_bf16x6"] = {"value": sig(em.get("value")), "x_f32": sig(em.get("speedup_vs_f32_simt"), 3),
@@ -743,11 +747,10 @@ def compact_line(full: dict) -> dict:
     bt = full.get("batched")
     if bt:
         line["batched"] = {"solves_per_s": sig(bt.get("solves_per_s")), "value": sig(bt.get("value")),
-                           "frac": sig(bt.get("frac"), 3), "x_full_gpu_loop": sig(bt.get("speedup_vs_full_gpu_loop"), 3),
-                           "resid_max": sig(bt.get("hpl_resid_flt_eps_max_sample"), 3)}
+                           "frac": sig(bt.get("frac"), 3), "x_full_gpu_loop": sig(bt.get("speedup_vs_full_gpu_loop"), 3)}
         if bt.get("bf16"):
             b16 = bt["bf16"]
-            line["batched"]["bf16"] = {"solves_per_s": sig(b16.get("solves_per_s")), "value": sig(b16.get("value")),
+            line["batched"]["bf16"] = {"solves_per_s": sig(b16.get("solves_per_s")),
                                        "iters": b16.get("ir_iters_max"), "hpl": sig(b16.get("hpl_resid_max"), 3),
                                        "err": sig(b16.get("max_rel_err_vs_fp64_sample"), 2)}
     sv = full.get("serving")
@@ -756,11 +759,15 @@ def compact_line(full: dict) -> dict:
         for p in ("f32", "bf16", "fp8"):
             eq = (sv.get(p) or {}).get("equal_p99")
             if eq:
-                line["serving"][p] = {"x_equal_p99": eq.get("ratio"), "p99_ms": sig(eq.get("p99_bound_ms"), 3),
-                                      "solves_per_s": eq.get("continuous_solves_per_s"),
-                                      "base": eq.get("baseline_solves_per_s")}
+                line["serving"][p] = {"x_equal_p99": eq.get("ratio"), "p99_ms": sig(eq.get("p99_bound_ms"), 3)}
     if full.get("details"):
         line["details"] = full["details"]
+    # the line must survive a stdout tail whole: drop the least central sections if it is long
+    for key in ("serving", "pivot", "fp64", "f32_bf16x6", "accuracy", "batched", "margins"):
+        if len(dumps_line(line)) <= LINE_LIMIT:
+            break
+        if line.pop(key, None) is not None:
+            line.setdefault("trimmed", []).append(key)
     return line
 
 

@@ -79,9 +79,13 @@ def test_compact_line_is_strict_small_and_complete():
     for k in ("value", "unit", "cores", "kind", "sample"):
         assert k in back["cpu_baseline"], k
     # every margin case carries its iteration count, HPL residual and oracle error
-    assert sum(len(v) for k, v in back["margins"].items() if k != "cols") == 12
+    rows = {k: v for k, v in back["margins"].items() if k not in ("cols", "margin")}
+    assert sum(len(v) for v in rows.values()) == 12
+    assert all(len(r) == len(back["margins"]["cols"]) for v in rows.values() for r in v)
+    assert all(len(back["margins"]["margin"][k.split()[0]]) == len(v) for k, v in rows.items())
     assert back["pivot"]["frac"] is None  # NaN became null, not an invalid token
     assert back["serving"]["bf16"]["x_equal_p99"] == 2.69
+    assert "trimmed" not in back  # nothing had to be dropped to fit
 
 
 def test_compact_line_with_legs_skipped():
@@ -102,3 +106,15 @@ def test_sig_rounding():
     assert bench.sig(math.nan) is None
     assert bench.sig(3) == 3
     assert bench.sig(None) is None
+
+
+def test_compact_line_trims_least_central_sections_when_long():
+    full = canned_full()
+    full["config"] = dict(full["config"], workload=full["config"]["workload"] + " " + "x" * 500)
+    line = bench.compact_line(full)
+    text = bench.dumps_line(line)
+    back = json.loads(text)
+    assert len(text.encode()) <= bench.LINE_LIMIT, len(text)
+    assert back["trimmed"][0] == "serving" and "serving" not in back
+    for k in REQUIRED:
+        assert k in back, k
