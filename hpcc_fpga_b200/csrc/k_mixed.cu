@@ -283,7 +283,8 @@ static int mixed_update(lp_ctx* c, float* c11, int lda, const uint8_t* aq, const
 //   left: each row l of the block column satisfies l_i = l0_i + sum_{k<i} l_k D_ki,
 //         i.e. l = l0 V with V = (I - strict-upper(D))^-1.
 // W^-1 and V are the two recurrences applied to a bs x bs identity (the exact
-// kernels, a small problem); then T = W^-1 T0 (into the zeroed block row) and
+// kernels over the nonzero triangle only, a small problem); then T = W^-1 T0
+// (into the zeroed block row) and
 // L += L (V - I) run as split-BF16 tensor-core products (nseg K-segments), so
 // the n bs^2 flops of the recurrences per step leave the FMA pipe.  V is unit
 // triangular, so L keeps its exact identity part; W^-1 is not (its diagonal
@@ -314,9 +315,9 @@ static int panel_tc(lp_ctx* c, float* dA, int n, int lda, int bs, int K, int nse
     LP_CUDA(cudaGetLastError());
     LP_CUDA(cudaEventRecord(c->ev_side, s));
     LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
-    LP_CHECK(left_blocked(d, lda, vinv, bs, bs, bs, vlt, bs, c->aux2));
+    LP_CHECK(left_blocked(d, lda, vinv, bs, bs, bs, vlt, bs, c->aux2, true));
     LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
-    LP_CHECK(top_blocked(c, d, lda, winv, bs, bs, bs, s));
+    LP_CHECK(top_blocked(c, d, lda, winv, bs, bs, bs, s, true));
     LP_CUDA(cudaStreamWaitEvent(s, c->ev_side_done, 0));
     k_add_diag<<<(bs + 127) / 128, 128, 0, s>>>(vinv, bs, -1.0f);
     count_launch();

@@ -158,19 +158,22 @@ int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
 // (full width, every column strip in parallel), then the chunk's
 // contribution to the rows below as one GEMM, T[below] += D[below][chunk] *
 // T[chunk] (D's sub-block transposed into the k-major operand first).
-int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols,
-                       cudaStream_t st) {
+// unit (T0 = identity): column j stays zero above row j, so chunk kk only
+// touches columns below (kk + 1) * 128; the skipped entries are exact zeros.
+int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st,
+                bool unit) {
     if (bs <= 128) return launch_trsm_top(d, lda, t, ldt, bs, ncols, st);
     const int ib = 128;
     float* dt = static_cast<float*>(c->dsub.ptr) + (st == c->aux ? (size_t)ib * bs : 0);
     for (int kk = 0; kk < bs / ib; kk++) {
         const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
         float* tk = t + (size_t)kk * ib * ldt;
-        LP_CHECK(launch_trsm_top(dkk, lda, tk, ldt, ib, ncols, st));
+        const int cols = unit ? std::min(ncols, (kk + 1) * ib) : ncols;
+        LP_CHECK(launch_trsm_top(dkk, lda, tk, ldt, ib, cols, st));
         const int m2 = bs - (kk + 1) * ib;
         if (m2 <= 0) break;
         LP_CHECK(launch_transpose(dkk + (size_t)ib * lda, lda, dt, m2, m2, ib, st));
-        LP_CHECK(launch_sgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, ncols, ib, st));
+        LP_CHECK(launch_sgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, cols, ib, st));
     }
     return LP_OK;
 }
@@ -179,18 +182,21 @@ int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, i
 // d, and Lt = L^T.  Larger blocks walk 128-column chunks: exact recurrence on
 // the chunk's columns (which also writes the chunk's rows of Lt), then
 // L[:, after] += L[:, chunk] * D[chunk][after] as one GEMM.
+// unit (L0 = identity): row i stays zero left of column i, so chunk kk only
+// touches rows above (kk + 1) * 128 (and only those rows of lt are written).
 int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
-                        cudaStream_t st) {
+                 cudaStream_t st, bool unit) {
     if (bs <= 128) return launch_trsm_left(d, lda, l, ldl, bs, nrows, lt, ldlt, st);
     const int ib = 128;
     for (int kk = 0; kk < bs / ib; kk++) {
         const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
         float* lk = l + (size_t)kk * ib;
         float* ltk = lt + (size_t)kk * ib * ldlt;
-        LP_CHECK(launch_trsm_left(dkk, lda, lk, ldl, ib, nrows, ltk, ldlt, st));
+        const int rows = unit ? std::min(nrows, (kk + 1) * ib) : nrows;
+        LP_CHECK(launch_trsm_left(dkk, lda, lk, ldl, ib, rows, ltk, ldlt, st));
         const int m2 = bs - (kk + 1) * ib;
         if (m2 <= 0) break;
-        LP_CHECK(launch_sgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, nrows, m2, ib, st));
+        LP_CHECK(launch_sgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, rows, m2, ib, st));
     }
     return LP_OK;
 }

@@ -46,6 +46,11 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
+// 16-byte copy (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async_vec16(void* smem, const void* gmem) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_elem(float* smem, const float* gmem) { cp_async4(smem, gmem); }
 __device__ __forceinline__ void cp_async_elem(double* smem, const double* gmem) { cp_async8(smem, gmem); }
 

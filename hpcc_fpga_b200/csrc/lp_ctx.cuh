@@ -46,10 +46,15 @@ inline int kseg(int k) { return (k + 511) / 512; }
 int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, int cols_t, int k, uint8_t* aq,
                 uint8_t* bq, cudaStream_t st, int nseg = 6);
 // The stages of panel_f32 (lp_abi.cu): lu of a diagonal block, and the top /
-// left recurrences over a block row / column (Lt written into lt).
+// left recurrences over a block row / column (Lt written into lt).  With
+// `unit` the operand is the bs x bs identity: top then yields a lower and left
+// an upper triangle, and each 128-wide chunk skips the columns (top) or rows
+// (left) that stay exactly zero.
 int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st);
-int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st);
-int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, cudaStream_t st);
+int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st,
+                bool unit = false);
+int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, cudaStream_t st,
+                 bool unit = false);
 // E4M3 scales: scale_x[seg * sstride + block] per 512-wide K segment and
 // 512-row (A) / 512-column (B) block (k_umma.cu).
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
