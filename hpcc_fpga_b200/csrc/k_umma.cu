@@ -846,9 +846,12 @@ int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const voi
     LP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // Leave a few SMs to the look-ahead panel on the auxiliary stream: one CTA
     // of this kernel fills an SM (shared memory, registers), so a full-width
-    // persistent grid would hold the panel off until the update ends
-    // (measured on B200, n = 32768: 8 free SMs +9 %; 16 to 48 no further gain).
-    constexpr int kPanelSMs = 8;
+    // persistent grid would hold the panel off until the update ends.  Measured
+    // on B200 (BF16 factorization alone): block 512, n = 32768: 8 free SMs +9 %
+    // over none; block 1024, n = 32768: 16 instead of 8 56.7 -> 55.3 ms (E4M3
+    // 63.9 -> 59.3 ms), 24 to 48 no further gain; block 2048, n = 65536, and the
+    // emulated FP32 form: 8 and 16 alike.
+    constexpr int kPanelSMs = 16;
     const int usable = sms - kPanelSMs > 1 ? sms - kPanelSMs : 1;
     if (pair) {
         const int tiles_n = n / 256, tiles = tiles_n * (m / 256);
