@@ -131,7 +131,7 @@ static double inner_bytes(double m, double n, double k) { return 4.0 * (2.0 * m 
 // Larger blocks are factored as the same blocked algorithm with 128-wide
 // inner blocks (lu, top, left, inner on the bs x bs sub-matrix), which keeps
 // every piece on the kernels above and spreads the inner work over the GPU.
-int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
+int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st, const TriInverses* inv) {
     if (bs <= 128) return launch_lu_small(d, lda, bs, st);
     const int ib = 128;
     float* lti = static_cast<float*>(c->lti.ptr);
@@ -139,15 +139,32 @@ int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
         float* dd = d + (size_t)kk * ib * lda + (size_t)kk * ib;
         LP_CHECK(launch_lu_small(dd, lda, ib, st));
         const int r = bs - (kk + 1) * ib;
-        if (r <= 0) break;
-        // top on st, left beside it on aux2 (both read only the factored block)
-        LP_CUDA(cudaEventRecord(c->ev_side, st));
-        LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
-        LP_CHECK(launch_trsm_top(dd, lda, dd + ib, lda, ib, r, st));
-        LP_CHECK(launch_trsm_left(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, c->aux2));
-        LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
-        LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
-        LP_CHECK(launch_sgemm_update(dd + (size_t)ib * lda + ib, lda, lti, r, dd + ib, lda, r, r, ib, st));
+        if (r > 0) {
+            // top on st, left beside it on aux2 (both read only the factored block)
+            LP_CUDA(cudaEventRecord(c->ev_side, st));
+            LP_CUDA(cudaStreamWaitEvent(c->aux2, c->ev_side, 0));
+            LP_CHECK(launch_trsm_top(dd, lda, dd + ib, lda, ib, r, st));
+            LP_CHECK(launch_trsm_left(dd, lda, dd + (size_t)ib * lda, lda, ib, r, lti, r, c->aux2));
+            LP_CUDA(cudaEventRecord(c->ev_side_done, c->aux2));
+            LP_CUDA(cudaStreamWaitEvent(st, c->ev_side_done, 0));
+        }
+        if (inv != nullptr) {
+            // block row and column kk of d are final (the trailing update below
+            // touches only rows and columns after them): chunk kk of the two
+            // identity recurrences, which read nothing else of d
+            LP_CUDA(cudaEventRecord(c->ev_inv[kk], st));
+            LP_CUDA(cudaStreamWaitEvent(c->inv_top, c->ev_inv[kk], 0));
+            LP_CUDA(cudaStreamWaitEvent(c->inv_left, c->ev_inv[kk], 0));
+            LP_CHECK(top_chunk_step(c, d, lda, inv->winv, bs, bs, bs, kk, c->inv_top, true));
+            LP_CHECK(left_chunk_step(d, lda, inv->vinv, bs, bs, bs, inv->vlt, bs, kk, c->inv_left, true));
+        }
+        if (r > 0) LP_CHECK(launch_sgemm_update(dd + (size_t)ib * lda + ib, lda, lti, r, dd + ib, lda, r, r, ib, st));
+    }
+    if (inv != nullptr) {
+        LP_CUDA(cudaEventRecord(c->ev_inv_top, c->inv_top));
+        LP_CUDA(cudaEventRecord(c->ev_inv_left, c->inv_left));
+        LP_CUDA(cudaStreamWaitEvent(st, c->ev_inv_top, 0));
+        LP_CUDA(cudaStreamWaitEvent(st, c->ev_inv_left, 0));
     }
     return LP_OK;
 }
@@ -160,21 +177,24 @@ int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st) {
 // T[chunk] (D's sub-block transposed into the k-major operand first).
 // unit (T0 = identity): column j stays zero above row j, so chunk kk only
 // touches columns below (kk + 1) * 128; the skipped entries are exact zeros.
+int top_chunk_step(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, int kk, cudaStream_t st,
+                   bool unit) {
+    const int ib = 128;
+    float* dt = static_cast<float*>(c->dsub.ptr) + (st == c->aux ? (size_t)ib * bs : 0);
+    const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+    float* tk = t + (size_t)kk * ib * ldt;
+    const int cols = unit ? std::min(ncols, (kk + 1) * ib) : ncols;
+    LP_CHECK(launch_trsm_top(dkk, lda, tk, ldt, ib, cols, st));
+    const int m2 = bs - (kk + 1) * ib;
+    if (m2 <= 0) return LP_OK;
+    LP_CHECK(launch_transpose(dkk + (size_t)ib * lda, lda, dt, m2, m2, ib, st));
+    return launch_sgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, cols, ib, st);
+}
+
 int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st,
                 bool unit) {
     if (bs <= 128) return launch_trsm_top(d, lda, t, ldt, bs, ncols, st);
-    const int ib = 128;
-    float* dt = static_cast<float*>(c->dsub.ptr) + (st == c->aux ? (size_t)ib * bs : 0);
-    for (int kk = 0; kk < bs / ib; kk++) {
-        const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
-        float* tk = t + (size_t)kk * ib * ldt;
-        const int cols = unit ? std::min(ncols, (kk + 1) * ib) : ncols;
-        LP_CHECK(launch_trsm_top(dkk, lda, tk, ldt, ib, cols, st));
-        const int m2 = bs - (kk + 1) * ib;
-        if (m2 <= 0) break;
-        LP_CHECK(launch_transpose(dkk + (size_t)ib * lda, lda, dt, m2, m2, ib, st));
-        LP_CHECK(launch_sgemm_update(tk + (size_t)ib * ldt, ldt, dt, m2, tk, ldt, m2, cols, ib, st));
-    }
+    for (int kk = 0; kk < bs / 128; kk++) LP_CHECK(top_chunk_step(c, d, lda, t, ldt, bs, ncols, kk, st, unit));
     return LP_OK;
 }
 
@@ -184,20 +204,23 @@ int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, i
 // L[:, after] += L[:, chunk] * D[chunk][after] as one GEMM.
 // unit (L0 = identity): row i stays zero left of column i, so chunk kk only
 // touches rows above (kk + 1) * 128 (and only those rows of lt are written).
+int left_chunk_step(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, int kk,
+                    cudaStream_t st, bool unit) {
+    const int ib = 128;
+    const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
+    float* lk = l + (size_t)kk * ib;
+    float* ltk = lt + (size_t)kk * ib * ldlt;
+    const int rows = unit ? std::min(nrows, (kk + 1) * ib) : nrows;
+    LP_CHECK(launch_trsm_left(dkk, lda, lk, ldl, ib, rows, ltk, ldlt, st));
+    const int m2 = bs - (kk + 1) * ib;
+    if (m2 <= 0) return LP_OK;
+    return launch_sgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, rows, m2, ib, st);
+}
+
 int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt,
                  cudaStream_t st, bool unit) {
     if (bs <= 128) return launch_trsm_left(d, lda, l, ldl, bs, nrows, lt, ldlt, st);
-    const int ib = 128;
-    for (int kk = 0; kk < bs / ib; kk++) {
-        const float* dkk = d + (size_t)kk * ib * lda + (size_t)kk * ib;
-        float* lk = l + (size_t)kk * ib;
-        float* ltk = lt + (size_t)kk * ib * ldlt;
-        const int rows = unit ? std::min(nrows, (kk + 1) * ib) : nrows;
-        LP_CHECK(launch_trsm_left(dkk, lda, lk, ldl, ib, rows, ltk, ldlt, st));
-        const int m2 = bs - (kk + 1) * ib;
-        if (m2 <= 0) break;
-        LP_CHECK(launch_sgemm_update(lk + ib, ldl, ltk, ldlt, dkk + ib, lda, rows, m2, ib, st));
-    }
+    for (int kk = 0; kk < bs / 128; kk++) LP_CHECK(left_chunk_step(d, lda, l, ldl, bs, nrows, lt, ldlt, kk, st, unit));
     return LP_OK;
 }
 
@@ -569,6 +592,12 @@ int lp_ctx_create(int device, lp_ctx** out) {
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->lane_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->lane_join, cudaEventDisableTiming);
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->inv_top, cudaStreamNonBlocking, prio_hi);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->inv_left, cudaStreamNonBlocking, prio_hi);
+    for (int i = 0; i < kMixedMaxBlock / 128 && e == cudaSuccess; i++)
+        e = cudaEventCreateWithFlags(&c->ev_inv[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_inv_top, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_inv_left, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         lp_ctx_destroy(c);
         return cuda_fail(e, "lp_ctx_create: stream/event creation", __FILE__, __LINE__);
@@ -587,7 +616,15 @@ int lp_ctx_destroy(lp_ctx* c) {
     if (c->copy_in != nullptr) cudaStreamSynchronize(c->copy_in);
     if (c->lane_st != nullptr) cudaStreamSynchronize(c->lane_st);
     if (c->lane_aux != nullptr) cudaStreamSynchronize(c->lane_aux);
+    if (c->inv_top != nullptr) cudaStreamSynchronize(c->inv_top);
+    if (c->inv_left != nullptr) cudaStreamSynchronize(c->inv_left);
     c->release_all();
+    for (int i = 0; i < kMixedMaxBlock / 128; i++)
+        if (c->ev_inv[i] != nullptr) cudaEventDestroy(c->ev_inv[i]);
+    if (c->ev_inv_top != nullptr) cudaEventDestroy(c->ev_inv_top);
+    if (c->ev_inv_left != nullptr) cudaEventDestroy(c->ev_inv_left);
+    if (c->inv_top != nullptr) cudaStreamDestroy(c->inv_top);
+    if (c->inv_left != nullptr) cudaStreamDestroy(c->inv_left);
     for (int i = 0; i < 8; i++)
         if (c->ev[i] != nullptr) cudaEventDestroy(c->ev[i]);
     if (c->ev_fork != nullptr) cudaEventDestroy(c->ev_fork);

@@ -50,11 +50,27 @@ int split_panel(const float* L, int ldl, const float* T, int ldt, int rows_l, in
 // `unit` the operand is the bs x bs identity: top then yields a lower and left
 // an upper triangle, and each 128-wide chunk skips the columns (top) or rows
 // (left) that stay exactly zero.
-int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st);
+// Inverses of the diagonal block's two triangles for the tensor-core panel:
+// top applied to the bs x bs identity (winv) and left applied to it (vinv;
+// vlt: scratch for its transposed chunks), both starting from the identity.
+struct TriInverses {
+    float* winv;
+    float* vinv;
+    float* vlt;
+};
+// With inv (bs > 128), chunk kk of both identity recurrences runs on the
+// context's inv_top / inv_left streams as soon as step kk of the lu stage has
+// made block row and column kk of d final; st waits for both at the end.
+int lu_stage(lp_ctx* c, float* d, int lda, int bs, cudaStream_t st, const TriInverses* inv = nullptr);
 int top_blocked(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, cudaStream_t st,
                 bool unit = false);
 int left_blocked(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, cudaStream_t st,
                  bool unit = false);
+// Step kk (128-wide chunk) of top_blocked / left_blocked, for bs > 128.
+int top_chunk_step(lp_ctx* c, const float* d, int lda, float* t, int ldt, int bs, int ncols, int kk, cudaStream_t st,
+                   bool unit);
+int left_chunk_step(const float* d, int lda, float* l, int ldl, int bs, int nrows, float* lt, int ldlt, int kk,
+                    cudaStream_t st, bool unit);
 // E4M3 scales: scale_x[seg * sstride + block] per 512-wide K segment and
 // 512-row (A) / 512-column (B) block (k_umma.cu).
 int launch_umma_update(float* c, int ldc, const void* aq, int aq_rows, const void* bq, int bq_rows, int m_off,
@@ -140,6 +156,12 @@ struct lp_ctx {
     cudaEvent_t ev_side = nullptr, ev_side_done = nullptr;
     cudaEvent_t ev_block = nullptr;           // blocking-sync event: waits yield the CPU instead of spinning
     cudaEvent_t ev[8] = {nullptr};
+    // tensor-core panel: the identity recurrences (inverses of the diagonal
+    // block's triangles) run on these two streams beside the lu stage, 128
+    // rows / columns behind it; ev_inv[kk]: step kk of the lu stage is final
+    cudaStream_t inv_top = nullptr, inv_left = nullptr;
+    cudaEvent_t ev_inv[lp::kMixedMaxBlock / 128] = {nullptr};
+    cudaEvent_t ev_inv_top = nullptr, ev_inv_left = nullptr;
     lp::Workspace lt;    // transposed left panels (2 x bs x n, alternating by block step)
     lp::Workspace dsub;  // transposed diagonal sub-blocks of the blocked top stage (per stream)
     lp::Workspace lti;   // transposed inner left panel of the recursive lu stage (per stream)
